@@ -1,0 +1,171 @@
+/*
+ * restir-b200: the frame driver, a C++ replacement of the reference's
+ * Renderer (src/renderer.h:73-125, src/renderer.cpp:435-1166) over the pass
+ * ABI of restir_gpu.h. It owns every device buffer of a frame and its
+ * history, derives each pass's uniforms exactly as Renderer::render does,
+ * and runs the passes in the reference's order on one CUDA stream
+ * (optionally replayed from a CUDA graph).
+ *
+ * Scope: the passes named in restir_gpu.h. TAA, auto exposure, tone
+ * mapping, specular GI and the debug views are not part of this driver;
+ * their settings are fixed off (TAA off also means the camera is jittered
+ * only while the reference accumulates, renderer.cpp:472-488).
+ */
+#ifndef RESTIR_FRAME_H
+#define RESTIR_FRAME_H
+
+#include "restir_gpu.h"
+#include "restir_host.h"
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The renderer's settings (src/settings.h:153-227), defaults from
+ * restir_settings_default. Enumerations as in settings.h: ray_mode 0 depth
+ * buffer, 1 hybrid, 2 BVH; direct_lighting 0 ReSTIR DI, 1 through GI only. */
+typedef struct RestirSettings
+{
+	float light_position[3];
+	float light_color[3];
+	float light_intensity;
+	int extra_lights;
+	float extra_intensity;
+	int extra_seed;
+	int sky_enabled;
+	float sky_zenith[3];
+	float sky_horizon[3];
+	float sky_ground[3];
+	float sky_intensity;
+	int multiple_bounces;
+	int shadows;
+	int denoiser;
+	int world_space_reuse;
+	int emissive_lighting;
+	int ray_mode;
+	int direct_lighting;
+	int clamp_jacobian;
+	int clamp_outliers;
+	int boiling_filter;
+	int gi_divisor;          /* 1, 2 or 4 (kGiResolutions) */
+	int shadow_face_size;    /* texels (kShadowFaceSizes: 256, 512, 1024, 2048) */
+	int atrous_iterations;   /* 0-5 */
+	int initial_candidates;
+	int temporal_taps;
+	int spatial_taps;
+	int trace_steps;
+	int di_candidates;
+	int di_spatial_taps;
+	uint32_t grid_table_size;
+	uint32_t grid_cell_capacity;
+	uint32_t grid_mode;      /* RESTIR_GRID_* */
+} RestirSettings;
+
+/* FrameInput (renderer.h) with the fly camera's pose. */
+typedef struct RestirFrameInput
+{
+	uint32_t width, height;
+	float eye[3];
+	float yaw, pitch;
+} RestirFrameInput;
+
+/* What Renderer carries from frame to frame. */
+typedef struct RestirFrameState
+{
+	uint32_t frame_number;
+	int history_valid;
+	int di_valid;
+	float previous_view_proj[16];
+	float previous_eye[3];
+	int reference_accumulating;
+	uint32_t reference_frames;
+} RestirFrameState;
+
+/* Which passes the frame runs. */
+typedef struct RestirFramePlan
+{
+	int di_active;                /* ReSTIR DI on, lights and a BVH present */
+	int denoiser;                 /* variance + a-trous iterations */
+	int atrous_iterations;
+	int reference_accumulate;     /* the reference accumulates this frame */
+	uint32_t reference_weight_frames; /* frames in the mean before this one */
+	int surface_light_is_di;      /* GI reads the DI diffuse (else the G-buffer emission) */
+} RestirFramePlan;
+
+void restir_settings_default(RestirSettings* settings);
+
+/* The uniforms and the plan of one frame, from the settings, the scene's
+ * description, its light count and the carried state (renderer.cpp:435-731).
+ * Pure host arithmetic: no device work. */
+int restir_frame_params(const RestirSettings* settings, const RestirMeshDesc* scene, uint32_t light_count,
+	const RestirBvhDesc* bvh, const RestirFrameInput* input, const RestirFrameState* state,
+	RestirParams* params, RestirFramePlan* plan);
+
+/* Advances the carried state after a frame (renderer.cpp:1119-1124). */
+void restir_frame_advance(const RestirParams* params, const RestirFramePlan* plan, const RestirFrameInput* input,
+	RestirFrameState* state);
+
+/* --- the renderer ---------------------------------------------------------- */
+
+/* Per-pass device times of the last frame, in milliseconds (cudaEvent pairs
+ * on the renderer's stream; the reference's per-view GPU times, ui.cpp:20-66). */
+#define RESTIR_PASS_SHADOW 0
+#define RESTIR_PASS_GBUFFER 1
+#define RESTIR_PASS_DI_TEMPORAL 2
+#define RESTIR_PASS_DI_SPATIAL 3
+#define RESTIR_PASS_GRID 4
+#define RESTIR_PASS_GI_TEMPORAL 5
+#define RESTIR_PASS_GI_SPATIAL 6
+#define RESTIR_PASS_DENOISE 7
+#define RESTIR_PASS_COMPOSITE 8
+#define RESTIR_PASS_REFERENCE 9
+#define RESTIR_PASS_COUNT 10
+
+typedef struct RestirMetrics
+{
+	int valid;
+	double relative_mse;          /* ReferenceMetrics::m_relativeMse */
+	double bias;                  /* mean image / mean reference - 1 */
+	double error[4];              /* the error pass's record */
+	float pass_ms[RESTIR_PASS_COUNT];
+	uint32_t reference_frames;
+} RestirMetrics;
+
+/* Creates a renderer on the current CUDA device, with its own stream. */
+void* restir_renderer_create(const RestirSettings* settings);
+void restir_renderer_destroy(void* renderer);
+/* Builds the BVH and light list on the host and uploads them
+ * (Renderer::setScene, renderer.cpp:365-419). Takes the light position and
+ * sky from the scene when use_scene_defaults is set (main.cpp:539-565). */
+int restir_renderer_set_scene(void* renderer, void* mesh, int use_scene_defaults);
+int restir_renderer_set_settings(void* renderer, const RestirSettings* settings);
+int restir_renderer_get_settings(void* renderer, RestirSettings* settings);
+/* Renders one frame (Renderer::render). The work is enqueued on the
+ * renderer's stream; the call returns without waiting for it. */
+int restir_renderer_render(void* renderer, const RestirFrameInput* input);
+/* Records one frame into a CUDA graph on first use and replays it after:
+ * the same as restir_renderer_render for inputs of the same size. */
+int restir_renderer_render_graph(void* renderer, const RestirFrameInput* input);
+/* Runs the error pass against the reference on the last frame and reads its
+ * record back (waits for the stream), as Renderer::frameSubmitted does. */
+int restir_renderer_measure(void* renderer, RestirMetrics* metrics);
+void restir_renderer_set_reference_accumulation(void* renderer, int accumulate);
+void restir_renderer_invalidate_history(void* renderer);
+/* Waits for the renderer's stream. */
+int restir_renderer_synchronize(void* renderer);
+/* The renderer's stream (a cudaStream_t). */
+void* restir_renderer_stream(void* renderer);
+/* The last frame's uniforms, plan and carried state. */
+int restir_renderer_last_frame(void* renderer, RestirParams* params, RestirFramePlan* plan, RestirFrameState* state);
+
+/* Device buffers of the renderer, by name ("hdr", "gbuffer.depth",
+ * "gi.sample", "grid", "reference.mean", ...): pointer and byte size. */
+int restir_renderer_buffer(void* renderer, const char* name, void** pointer, uint64_t* bytes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RESTIR_FRAME_H */

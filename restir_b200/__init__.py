@@ -1,0 +1,255 @@
+"""restir-b200: B200-native per-frame light transport of the pkonecki/restir renderer.
+
+The product is librestir_gpu.so (hand-written sm_100a CUDA kernels behind the
+C ABI of include/restir_gpu.h, and the C++ frame driver and scene preparation
+of include/restir_frame.h and include/restir_host.h). This module loads it
+through ctypes and mirrors the reference renderer's interface
+(src/renderer.h:73-125: init, setScene, render, invalidateHistory,
+setReferenceAccumulation, frameSubmitted / metrics) for Python callers.
+
+There is no CPU fallback: every call that computes goes to the CUDA library,
+and loading fails loudly when the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+from . import abi
+from .abi import (RestirBvhDesc, RestirDiReservoirs, RestirFrameInput, RestirFramePlan, RestirFrameState,
+                  RestirGBuffer, RestirGiHistory, RestirGiReservoirs, RestirLightsDesc, RestirMeshDesc,
+                  RestirParams, RestirScene, RestirSettings)
+
+LIBRARY_PATH = Path(__file__).resolve().parent / "librestir_gpu.so"
+
+SCENE_CORNELL, SCENE_COURTYARD, SCENE_CITY = 0, 1, 2
+GRID_ATOMIC, GRID_DETERMINISTIC = 0, 1
+RAY_SCREEN, RAY_HYBRID, RAY_BVH = 0, 1, 2
+TRACE_CLOSEST, TRACE_ANY, TRACE_CLOSEST_STACKLESS, TRACE_CLOSEST_WATERTIGHT = 0, 1, 2, 3
+PASS_NAMES = ["shadow", "gbuffer", "di_temporal", "di_spatial", "grid", "gi_temporal", "gi_spatial",
+              "denoise", "composite", "reference"]
+
+_lib = None
+
+P = C.c_void_p
+u32 = C.c_uint32
+i32 = C.c_int32
+
+_SIGNATURES = {
+    # restir_gpu.h
+    "restir_trace": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirScene), P, P, P, u32, C.c_int, P]),
+    "restir_shadow_atlas": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirScene), P, P]),
+    "restir_gbuffer_primary": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirScene), C.POINTER(RestirGBuffer), P]),
+    "restir_grid_clear": (C.c_int, [C.POINTER(RestirParams), P, P]),
+    "restir_grid_insert": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirGBuffer), P, P]),
+    "restir_di_temporal": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirScene), C.POINTER(RestirGBuffer),
+                                     C.POINTER(RestirDiReservoirs), C.POINTER(RestirDiReservoirs), P]),
+    "restir_di_spatial": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirScene), C.POINTER(RestirGBuffer),
+                                    C.POINTER(RestirDiReservoirs), P, P, P]),
+    "restir_gi_temporal": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirScene), C.POINTER(RestirGBuffer),
+                                     C.POINTER(RestirGiHistory), P, P, P, C.POINTER(RestirGiReservoirs), P]),
+    "restir_gi_spatial": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirScene), C.POINTER(RestirGBuffer),
+                                    C.POINTER(RestirGiReservoirs), P, C.POINTER(RestirGiHistory), P, P, P, P, P]),
+    "restir_svgf_variance": (C.c_int, [C.POINTER(RestirParams), P, P, P, P, P, P]),
+    "restir_svgf_atrous": (C.c_int, [C.POINTER(RestirParams), C.c_int, P, P, P, P, P]),
+    "restir_composite": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirGBuffer), P, P, P, P, P, P]),
+    "restir_reference_accumulate": (C.c_int, [C.POINTER(RestirParams), P, P, P, u32, P]),
+    "restir_error_scratch_bytes": (C.c_uint64, [u32, u32]),
+    "restir_error": (C.c_int, [C.POINTER(RestirParams), P, P, P, P, P, P]),
+    "restir_status": (C.c_int, [C.POINTER(u32)]),
+    "restir_numeric_eval": (C.c_int, [C.c_int, P, P, u32, P]),
+    # restir_host.h
+    "restir_mesh_procedural": (P, [C.c_int, u32, u32]),
+    "restir_mesh_create": (P, [C.POINTER(RestirMeshDesc)]),
+    "restir_mesh_describe": (C.c_int, [P, C.POINTER(RestirMeshDesc)]),
+    "restir_mesh_destroy": (None, [P]),
+    "restir_bvh_build": (P, [C.POINTER(RestirMeshDesc), C.c_int]),
+    "restir_bvh_describe": (C.c_int, [P, C.POINTER(RestirBvhDesc)]),
+    "restir_bvh_destroy": (None, [P]),
+    "restir_lights_build": (P, [P, C.c_int, C.c_int, C.c_float, u32, P, P, C.c_float]),
+    "restir_lights_describe": (C.c_int, [P, C.POINTER(RestirLightsDesc)]),
+    "restir_lights_destroy": (None, [P]),
+    "restir_camera_matrices": (None, [P, C.c_float, C.c_float, C.c_float, P, C.c_float, P, P]),
+    # restir_frame.h
+    "restir_settings_default": (None, [C.POINTER(RestirSettings)]),
+    "restir_frame_params": (C.c_int, [C.POINTER(RestirSettings), C.POINTER(RestirMeshDesc), u32,
+                                      C.POINTER(RestirBvhDesc), C.POINTER(RestirFrameInput),
+                                      C.POINTER(RestirFrameState), C.POINTER(RestirParams),
+                                      C.POINTER(RestirFramePlan)]),
+    "restir_frame_advance": (None, [C.POINTER(RestirParams), C.POINTER(RestirFramePlan), C.POINTER(RestirFrameInput),
+                                    C.POINTER(RestirFrameState)]),
+}
+
+# Entry points that may be absent while the library is being extended.
+_OPTIONAL = {"restir_di_temporal", "restir_di_spatial", "restir_gi_temporal", "restir_gi_spatial",
+             "restir_svgf_variance", "restir_svgf_atrous", "restir_composite", "restir_reference_accumulate",
+             "restir_error_scratch_bytes", "restir_error"}
+
+
+def load() -> C.CDLL:
+    """The CUDA library. Raises if it has not been built (python -m restir_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not LIBRARY_PATH.exists():
+            raise RuntimeError(f"{LIBRARY_PATH} is missing: build it with `python -m restir_b200.build`")
+        lib = C.CDLL(str(LIBRARY_PATH))
+        for name, (restype, argtypes) in _SIGNATURES.items():
+            if not hasattr(lib, name):
+                if name in _OPTIONAL:
+                    continue
+                raise RuntimeError(f"{LIBRARY_PATH} does not export {name}")
+            fn = getattr(lib, name)
+            fn.restype = restype
+            fn.argtypes = argtypes
+        _lib = lib
+    return _lib
+
+
+def ptr(x) -> int | None:
+    """Address of a torch tensor, numpy array, ctypes object or int (None for None)."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    if isinstance(x, np.ndarray):
+        return x.ctypes.data
+    return C.addressof(x)
+
+
+def check(status: int, what: str) -> None:
+    if status != 0:
+        raise RuntimeError(f"{what} failed with status {status}")
+
+
+# --- host scene preparation ------------------------------------------------------------------------
+
+
+class Mesh:
+    """A triangle soup (restir_host.h): procedural or from arrays."""
+
+    def __init__(self, handle: int):
+        if not handle:
+            raise RuntimeError("mesh creation failed")
+        self.handle = handle
+        self.desc = RestirMeshDesc()
+        check(load().restir_mesh_describe(handle, C.byref(self.desc)), "restir_mesh_describe")
+
+    @classmethod
+    def procedural(cls, kind: int, seed: int = 0, triangles: int = 0) -> "Mesh":
+        return cls(load().restir_mesh_procedural(kind, seed, triangles))
+
+    @property
+    def triangle_count(self) -> int:
+        return self.desc.triangle_count
+
+    def positions(self) -> np.ndarray:
+        return np.ctypeslib.as_array(C.cast(self.desc.positions, C.POINTER(C.c_float)),
+                                     (self.triangle_count * 9,)).copy()
+
+    def __del__(self):
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.restir_mesh_destroy(self.handle)
+            self.handle = None
+
+
+class Bvh:
+    """The reference layout (src/bvh.h) built by this library's host builder."""
+
+    def __init__(self, mesh: Mesh, threads: int = 0):
+        threads = threads or (os.cpu_count() or 1)
+        self.handle = load().restir_bvh_build(C.byref(mesh.desc), threads)
+        if not self.handle:
+            raise RuntimeError("restir_bvh_build failed")
+        self.desc = RestirBvhDesc()
+        check(load().restir_bvh_describe(self.handle, C.byref(self.desc)), "restir_bvh_describe")
+        d = self.desc
+        fp = C.POINTER(C.c_float)
+        self.data = np.ctypeslib.as_array(C.cast(d.data, fp), (d.float_count,)).copy()
+        n = d.triangle_count
+        self.triangle_normals = np.ctypeslib.as_array(C.cast(d.triangle_normals, fp), (n * 4,)).copy() if n else \
+            np.zeros(0, np.float32)
+        self.order = np.ctypeslib.as_array(C.cast(d.order, C.POINTER(C.c_uint32)), (n,)).copy() if n else \
+            np.zeros(0, np.uint32)
+
+    def __del__(self):
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.restir_bvh_destroy(self.handle)
+            self.handle = None
+
+
+class Lights:
+    """The DI light list (src/lights.h layout)."""
+
+    def __init__(self, bvh: Bvh, mesh: Mesh, settings: RestirSettings, include_emitters: bool = True):
+        radius = mesh.desc.radius
+        scale = (radius / 1.75) ** 2
+        lo = (C.c_float * 3)(*mesh.desc.bounds_min)
+        hi = (C.c_float * 3)(*mesh.desc.bounds_max)
+        self.handle = load().restir_lights_build(bvh.handle, int(include_emitters and settings.emissive_lighting),
+                                                 settings.extra_lights, settings.extra_intensity,
+                                                 settings.extra_seed, lo, hi, scale)
+        desc = RestirLightsDesc()
+        check(load().restir_lights_describe(self.handle, C.byref(desc)), "restir_lights_describe")
+        self.count = desc.count
+        self.triangles = desc.triangles
+        self.data = np.ctypeslib.as_array(C.cast(desc.data, C.POINTER(C.c_float)), (desc.count * 16,)).copy() \
+            if desc.count else np.zeros(16, np.float32)
+
+    def __del__(self):
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.restir_lights_destroy(self.handle)
+            self.handle = None
+
+
+def default_settings(mesh: Mesh | None = None) -> RestirSettings:
+    """Settings defaults (settings.h:183-227), with the scene's light and sky when given (main.cpp:539-565)."""
+    s = RestirSettings()
+    load().restir_settings_default(C.byref(s))
+    if mesh is not None:
+        for k in range(3):
+            s.light_position[k] = mesh.desc.light_position[k]
+        s.sky_enabled = mesh.desc.sky
+    return s
+
+
+def frame_params(settings: RestirSettings, mesh: Mesh, light_count: int, bvh: Bvh, frame_input: RestirFrameInput,
+                 state: RestirFrameState) -> tuple[RestirParams, RestirFramePlan]:
+    params = RestirParams()
+    plan = RestirFramePlan()
+    check(load().restir_frame_params(C.byref(settings), C.byref(mesh.desc), light_count, C.byref(bvh.desc),
+                                     C.byref(frame_input), C.byref(state), C.byref(params), C.byref(plan)),
+          "restir_frame_params")
+    return params, plan
+
+
+def initial_state() -> RestirFrameState:
+    state = RestirFrameState()
+    for i in range(4):
+        state.previous_view_proj[i * 5] = 1.0
+    return state
+
+
+def frame_input(mesh: Mesh, width: int, height: int, eye=None, yaw=None, pitch=None) -> RestirFrameInput:
+    fi = RestirFrameInput()
+    fi.width, fi.height = width, height
+    e = eye if eye is not None else mesh.desc.camera_eye
+    for k in range(3):
+        fi.eye[k] = e[k]
+    fi.yaw = mesh.desc.camera_yaw if yaw is None else yaw
+    fi.pitch = mesh.desc.camera_pitch if pitch is None else pitch
+    return fi
+
+
+def advance(params: RestirParams, plan: RestirFramePlan, frame_input: RestirFrameInput, state: RestirFrameState):
+    load().restir_frame_advance(C.byref(params), C.byref(plan), C.byref(frame_input), C.byref(state))
+
+
+def status_flags() -> int:
+    flags = C.c_uint32(0)
+    check(load().restir_status(C.byref(flags)), "restir_status")
+    return flags.value

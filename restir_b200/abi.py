@@ -1,0 +1,126 @@
+"""ctypes mirrors of the C structs in include/restir_gpu.h and include/restir_host.h.
+
+Field order and types must match the headers exactly; tests/test_abi.py checks
+the sizes against the compiled library.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+f4 = C.c_float * 4
+m16 = C.c_float * 16
+f3 = C.c_float * 3
+
+
+class RestirParams(C.Structure):
+    _fields_ = [
+        ("view_proj", m16), ("inv_view_proj", m16), ("prev_view_proj", m16),
+        ("shadow_view_proj", m16 * 6), ("shadow_inv_view_proj", m16 * 6),
+        ("light_position", f4), ("light_color", f4), ("camera_position", f4), ("prev_camera_position", f4),
+        ("frame_index", C.c_float), ("history_valid", C.c_float), ("origin_bottom_left", C.c_float),
+        ("multiple_bounces", C.c_float),
+        ("width", C.c_uint32), ("height", C.c_uint32), ("gi_width", C.c_uint32), ("gi_height", C.c_uint32),
+        ("scene_scale", C.c_float), ("boiling_filter", C.c_float), ("jacobian_clamp", C.c_float),
+        ("outlier_clamp", C.c_float),
+        ("surface_light_scale", C.c_float), ("emission_scale", C.c_float),
+        ("initial_candidates", C.c_int32), ("temporal_taps", C.c_int32), ("spatial_taps", C.c_int32),
+        ("trace_steps", C.c_int32),
+        ("grid_min_cell", C.c_float), ("grid_pixel_size", C.c_float), ("grid_cell_pixels", C.c_float),
+        ("world_space_reuse", C.c_float), ("grid_table_size", C.c_uint32), ("grid_cell_capacity", C.c_uint32),
+        ("grid_mode", C.c_uint32),
+        ("ray_mode", C.c_int32),
+        ("di_light_count", C.c_int32), ("di_candidates", C.c_int32), ("di_spatial_taps", C.c_int32),
+        ("di_history_valid", C.c_float),
+        ("shadow_far", C.c_float), ("shadow_tan_half_fov", C.c_float), ("shadow_inv_face_size", C.c_float),
+        ("shadows_enabled", C.c_float), ("shadow_face_size", C.c_uint32),
+        ("sky_zenith", f4), ("sky_horizon", f4), ("sky_ground", f4),
+        ("composite_options", f4),
+    ]
+
+
+class RestirScene(C.Structure):
+    _fields_ = [
+        ("bvh", C.c_void_p), ("node_count", C.c_uint32), ("triangle_offset", C.c_uint32),
+        ("triangle_count", C.c_uint32), ("lights", C.c_void_p), ("light_count", C.c_uint32),
+        ("triangle_normals", C.c_void_p), ("materials", C.c_void_p), ("material_count", C.c_uint32),
+    ]
+
+
+class RestirGBuffer(C.Structure):
+    _fields_ = [("albedo", C.c_void_p), ("normal", C.c_void_p), ("emissive", C.c_void_p),
+                ("shading_normal", C.c_void_p), ("depth", C.c_void_p)]
+
+
+class RestirGiReservoirs(C.Structure):
+    _fields_ = [("sample", C.c_void_p), ("receiver", C.c_void_p), ("normal", C.c_void_p)]
+
+
+class RestirGiHistory(C.Structure):
+    _fields_ = [("sample", C.c_void_p), ("receiver", C.c_void_p), ("normal", C.c_void_p),
+                ("color", C.c_void_p), ("moments", C.c_void_p)]
+
+
+class RestirDiReservoirs(C.Structure):
+    _fields_ = [("sample", C.c_void_p), ("receiver", C.c_void_p), ("normal", C.c_void_p)]
+
+
+class RestirMeshDesc(C.Structure):
+    _fields_ = [
+        ("triangle_count", C.c_uint32), ("positions", C.c_void_p), ("normals", C.c_void_p),
+        ("triangle_material", C.c_void_p), ("material_count", C.c_uint32), ("materials", C.c_void_p),
+        ("bounds_min", f3), ("bounds_max", f3), ("center", f3), ("radius", C.c_float),
+        ("light_position", f3), ("camera_eye", f3), ("camera_yaw", C.c_float), ("camera_pitch", C.c_float),
+        ("sky", C.c_int),
+    ]
+
+
+class RestirBvhDesc(C.Structure):
+    _fields_ = [
+        ("data", C.c_void_p), ("float_count", C.c_uint64), ("node_count", C.c_uint32),
+        ("triangle_offset", C.c_uint32), ("triangle_count", C.c_uint32), ("depth", C.c_uint32),
+        ("triangle_normals", C.c_void_p), ("order", C.c_void_p), ("emitter_count", C.c_uint32),
+        ("emitters", C.c_void_p), ("build_ms", C.c_double),
+    ]
+
+
+class RestirLightsDesc(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("count", C.c_uint32), ("triangles", C.c_uint32)]
+
+
+class RestirSettings(C.Structure):
+    _fields_ = [
+        ("light_position", f3), ("light_color", f3), ("light_intensity", C.c_float),
+        ("extra_lights", C.c_int), ("extra_intensity", C.c_float), ("extra_seed", C.c_int),
+        ("sky_enabled", C.c_int), ("sky_zenith", f3), ("sky_horizon", f3), ("sky_ground", f3),
+        ("sky_intensity", C.c_float),
+        ("multiple_bounces", C.c_int), ("shadows", C.c_int), ("denoiser", C.c_int),
+        ("world_space_reuse", C.c_int), ("emissive_lighting", C.c_int), ("ray_mode", C.c_int),
+        ("direct_lighting", C.c_int), ("clamp_jacobian", C.c_int), ("clamp_outliers", C.c_int),
+        ("boiling_filter", C.c_int),
+        ("gi_divisor", C.c_int), ("shadow_face_size", C.c_int), ("atrous_iterations", C.c_int),
+        ("initial_candidates", C.c_int), ("temporal_taps", C.c_int), ("spatial_taps", C.c_int),
+        ("trace_steps", C.c_int), ("di_candidates", C.c_int), ("di_spatial_taps", C.c_int),
+        ("grid_table_size", C.c_uint32), ("grid_cell_capacity", C.c_uint32), ("grid_mode", C.c_uint32),
+    ]
+
+
+class RestirFrameInput(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("eye", f3), ("yaw", C.c_float),
+                ("pitch", C.c_float)]
+
+
+class RestirFrameState(C.Structure):
+    _fields_ = [
+        ("frame_number", C.c_uint32), ("history_valid", C.c_int), ("di_valid", C.c_int),
+        ("previous_view_proj", m16), ("previous_eye", f3), ("reference_accumulating", C.c_int),
+        ("reference_frames", C.c_uint32),
+    ]
+
+
+class RestirFramePlan(C.Structure):
+    """Which passes a frame runs, as Renderer::render decides (renderer.cpp:627-1094)."""
+    _fields_ = [
+        ("di_active", C.c_int), ("denoiser", C.c_int), ("atrous_iterations", C.c_int),
+        ("reference_accumulate", C.c_int), ("reference_weight_frames", C.c_uint32),
+        ("surface_light_is_di", C.c_int),
+    ]

@@ -1,0 +1,87 @@
+"""Builds restir_b200/librestir_gpu.so in the source tree.
+
+CUDA sources (csrc/*.cu) are compiled for sm_100a only, as relocatable
+device code (they share the device status word), with --fmad=false and IEEE
+division and square root (include/restir_numeric.h); host sources
+(host/*.cpp) with -ffp-contract=off. Objects go to restir_b200/_build/ and are
+rebuilt when a source or header is newer. Run as `python -m restir_b200.build`.
+"""
+from __future__ import annotations
+
+import concurrent.futures
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PACKAGE = Path(__file__).resolve().parent
+ROOT = PACKAGE.parent
+CSRC = PACKAGE / "csrc"
+HOST = PACKAGE / "host"
+BUILD = PACKAGE / "_build"
+LIBRARY = PACKAGE / "librestir_gpu.so"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ARCH + [
+    "-O3", "-lineinfo", "-std=c++17", "-rdc=true",
+    "--fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
+    "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+    "-I", str(ROOT / "include"),
+]
+CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall",
+             "-I", str(ROOT / "include")]
+
+
+def _nvcc() -> str:
+    home = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+    candidate = Path(home) / "bin" / "nvcc"
+    return str(candidate) if candidate.exists() else (shutil.which("nvcc") or "nvcc")
+
+
+def _headers() -> list[Path]:
+    return sorted(CSRC.glob("*.cuh")) + sorted(HOST.glob("*.h")) + sorted((ROOT / "include").glob("*.h"))
+
+
+def _stale(target: Path, sources: list[Path]) -> bool:
+    if not target.exists():
+        return True
+    stamp = target.stat().st_mtime
+    return any(s.stat().st_mtime > stamp for s in sources)
+
+
+def _run(command: list[str]) -> None:
+    result = subprocess.run(command, capture_output=True, text=True)
+    if result.returncode != 0:
+        raise RuntimeError("build failed:\n" + " ".join(command) + "\n" + result.stdout + result.stderr)
+
+
+def build(verbose: bool = False) -> Path:
+    BUILD.mkdir(exist_ok=True)
+    nvcc = _nvcc()
+    headers = _headers()
+    jobs = []
+    objects = []
+    for source in sorted(CSRC.glob("*.cu")):
+        obj = BUILD / (source.stem + ".cu.o")
+        objects.append(obj)
+        if _stale(obj, [source] + headers):
+            jobs.append([nvcc] + NVCC_FLAGS + ["-c", str(source), "-o", str(obj)])
+    for source in sorted(HOST.glob("*.cpp")):
+        obj = BUILD / (source.stem + ".cpp.o")
+        objects.append(obj)
+        if _stale(obj, [source] + headers):
+            jobs.append(["g++"] + CXX_FLAGS + ["-c", str(source), "-o", str(obj)])
+    with concurrent.futures.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as pool:
+        for command in jobs:
+            if verbose:
+                print(" ".join(command), file=sys.stderr)
+        list(pool.map(_run, jobs))
+    if jobs or _stale(LIBRARY, objects):
+        _run([nvcc] + ARCH + ["-shared", "-rdc=true", "-Xcompiler", "-fPIC"] + [str(o) for o in objects]
+             + ["-o", str(LIBRARY), "-lcudart"])
+    return LIBRARY
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv))

@@ -1,0 +1,328 @@
+// BVH traversal over the reference's depth-first node layout (src/bvh.h:7-22):
+// node i = float4 rows 2i, 2i+1: (min.xyz, a), (max.xyz, b); b >= 0 a leaf of
+// triangles [a, a+b), b < 0 an interior node with right child a and skip
+// link -b-1; triangle t = rows triangleOffset + 4t .. +3.
+//
+// Same algorithms and arithmetic as shaders/bvh.sh (slab test 32-41,
+// Moeller-Trumbore 44-71, stackless walk 140-174, nearest-first short stack
+// 216-295), so hit ids and distances are bit-identical to the CPU
+// restatement. Every node and triangle row is one 16-byte read-only load.
+#pragma once
+
+#include "common.cuh"
+
+namespace restir
+{
+
+#define kBvhShortStack 8
+#define kBvhMaxSteps 2048
+
+struct BvhView
+{
+	const float4* rows = nullptr;
+	int nodeCount = 0;
+	int triangleOffset = 0;
+
+	__device__ __forceinline__ bool available() const { return nodeCount > 0; }
+	__device__ __forceinline__ V4 row(int i) const
+	{
+		float4 q = __ldg(rows + i);
+		return { q.x, q.y, q.z, q.w };
+	}
+	__device__ __forceinline__ V3 vertex(int t, int corner) const { return row(triangleOffset + t * 4 + corner).xyz(); }
+	__device__ __forceinline__ V3 albedo(int t) const { return row(triangleOffset + t * 4 + 3).xyz(); }
+	__device__ __forceinline__ V3 emission(int t) const
+	{
+		int base = triangleOffset + t * 4;
+		return v3(row(base + 1).w, row(base + 2).w, row(base + 3).w);
+	}
+};
+
+__host__ __device__ inline BvhView makeBvhView(const RestirScene* s)
+{
+	BvhView b;
+	if (s != nullptr && s->bvh != nullptr)
+	{
+		b.rows = reinterpret_cast<const float4*>(s->bvh);
+		b.nodeCount = int(s->node_count);
+		b.triangleOffset = int(s->triangle_offset);
+	}
+	return b;
+}
+
+__device__ __forceinline__ float intersectBox(V3 o, V3 inv, V3 bmin, V3 bmax, float maxDistance)
+{
+	V3 t0 = (bmin - o) * inv;
+	V3 t1 = (bmax - o) * inv;
+	V3 n = vmin(t0, t1);
+	V3 f = vmax(t0, t1);
+	float enter = fmaxf(fmaxf(n.x, n.y), fmaxf(n.z, 0.0f));
+	float leave = fminf(fminf(f.x, f.y), fminf(f.z, maxDistance));
+	return enter <= leave ? enter : -1.0f;
+}
+
+__device__ __forceinline__ float intersectTriangle(V3 o, V3 d, V3 v0, V3 v1, V3 v2)
+{
+	V3 edge1 = v1 - v0;
+	V3 edge2 = v2 - v0;
+	V3 p = cross(d, edge2);
+	float determinant = dot(edge1, p);
+	if (fabsf(determinant) < 1e-12f)
+	{
+		return -1.0f;
+	}
+	float inverse = 1.0f / determinant;
+	V3 s = o - v0;
+	float u = dot(s, p) * inverse;
+	if (u < 0.0f || u > 1.0f)
+	{
+		return -1.0f;
+	}
+	V3 q = cross(s, edge1);
+	float v = dot(d, q) * inverse;
+	if (v < 0.0f || u + v > 1.0f)
+	{
+		return -1.0f;
+	}
+	return dot(edge2, q) * inverse;
+}
+
+__device__ __forceinline__ float safeInverse(float d)
+{
+	float s = fabsf(d) > 1e-8f ? d : (d >= 0.0f ? 1e-8f : -1e-8f);
+	return 1.0f / s;
+}
+
+__device__ __forceinline__ V3 bvhInverseDirection(V3 d)
+{
+	return { safeInverse(d.x), safeInverse(d.y), safeInverse(d.z) };
+}
+
+__device__ __forceinline__ int intersectLeaf(const BvhView& b, V3 o, V3 d, int first, int count, float& distance, int hit)
+{
+	for (int t = first; t < first + count; ++t)
+	{
+		float h = intersectTriangle(o, d, b.vertex(t, 0), b.vertex(t, 1), b.vertex(t, 2));
+		if (h > 0.0f && h < distance)
+		{
+			distance = h;
+			hit = t;
+		}
+	}
+	return hit;
+}
+
+// bvh.sh:140-174
+__device__ inline int traceStackless(const BvhView& b, V3 o, V3 d, bool anyHit, float& distance)
+{
+	V3 inv = bvhInverseDirection(d);
+	int hit = -1;
+	int node = 0;
+	int step = 0;
+	for (; step < kBvhMaxSteps; ++step)
+	{
+		if (node >= b.nodeCount)
+		{
+			break;
+		}
+		V4 node0 = b.row(node * 2);
+		V4 node1 = b.row(node * 2 + 1);
+		bool leaf = node1.w >= 0.0f;
+		if (intersectBox(o, inv, node0.xyz(), node1.xyz(), distance) < 0.0f)
+		{
+			node = leaf ? node + 1 : int(-node1.w) - 1;
+			continue;
+		}
+		if (leaf)
+		{
+			hit = intersectLeaf(b, o, d, int(node0.w), int(node1.w), distance, hit);
+			if (anyHit && hit >= 0)
+			{
+				return hit;
+			}
+		}
+		node = node + 1;
+	}
+	if (step == kBvhMaxSteps)
+	{
+		raiseStatus(1u);
+	}
+	return hit;
+}
+
+// bvh.sh:216-295. stack: this thread's kBvhShortStack entries, stride apart
+// (shared memory, interleaved across the block's threads).
+__device__ inline int traceShortStack(const BvhView& b, V3 o, V3 d, float& distance, int* stack, int stride)
+{
+	V3 inv = bvhInverseDirection(d);
+	if (intersectBox(o, inv, b.row(0).xyz(), b.row(1).xyz(), distance) < 0.0f)
+	{
+		return -1;
+	}
+	int stackTop = 0;
+	int stackCount = 0;
+	bool dropped = false;
+	int hit = -1;
+	int node = 0;
+	int step = 0;
+	for (; step < kBvhMaxSteps; ++step)
+	{
+		V4 node0 = b.row(node * 2);
+		V4 node1 = b.row(node * 2 + 1);
+		if (node1.w >= 0.0f)
+		{
+			hit = intersectLeaf(b, o, d, int(node0.w), int(node1.w), distance, hit);
+		}
+		else
+		{
+			int left = node + 1;
+			int right = int(node0.w);
+			float leftDistance = intersectBox(o, inv, b.row(left * 2).xyz(), b.row(left * 2 + 1).xyz(), distance);
+			float rightDistance = intersectBox(o, inv, b.row(right * 2).xyz(), b.row(right * 2 + 1).xyz(), distance);
+			bool visitLeft = leftDistance >= 0.0f;
+			bool visitRight = rightDistance >= 0.0f;
+			if (visitLeft && visitRight)
+			{
+				bool leftFirst = leftDistance <= rightDistance;
+				stack[(stackTop & (kBvhShortStack - 1)) * stride] = leftFirst ? right : left;
+				++stackTop;
+				if (stackCount == kBvhShortStack)
+				{
+					dropped = true;
+				}
+				else
+				{
+					++stackCount;
+				}
+				node = leftFirst ? left : right;
+				continue;
+			}
+			if (visitLeft || visitRight)
+			{
+				node = visitLeft ? left : right;
+				continue;
+			}
+		}
+		if (stackCount == 0)
+		{
+			break;
+		}
+		--stackTop;
+		--stackCount;
+		node = stack[(stackTop & (kBvhShortStack - 1)) * stride];
+	}
+	if (step == kBvhMaxSteps)
+	{
+		raiseStatus(1u);
+	}
+	if (dropped)
+	{
+		int stacklessHit = traceStackless(b, o, d, false, distance);
+		if (stacklessHit >= 0)
+		{
+			hit = stacklessHit;
+		}
+	}
+	return hit;
+}
+
+// traceBvh (bvh.sh:298-319). stack == nullptr: stackless for every ray (the
+// passes without BVH_SHARED_STACK).
+__device__ __forceinline__ int traceBvh(const BvhView& b, V3 o, V3 d, float maxDistance, bool anyHit, float& distance,
+	int* stack, int stride)
+{
+	distance = maxDistance;
+	if (!b.available())
+	{
+		return -1;
+	}
+	if (stack != nullptr && !anyHit)
+	{
+		return traceShortStack(b, o, d, distance, stack, stride);
+	}
+	return traceStackless(b, o, d, anyHit, distance);
+}
+
+// Nearest hit in (0, distance) among the triangles accept() lets through,
+// ties to the lower triangle index, so the result does not depend on the
+// visiting order. A full stack of 64 entries in local memory, nearest child
+// first; the layout's depth is at most 40 (bvh.h:49), so it cannot overflow.
+template<typename Accept>
+__device__ inline int traceNearestFiltered(const BvhView& b, V3 o, V3 d, float& distance, Accept accept)
+{
+	V3 inv = bvhInverseDirection(d);
+	if (!b.available() || intersectBox(o, inv, b.row(0).xyz(), b.row(1).xyz(), distance) < 0.0f)
+	{
+		return -1;
+	}
+	int stack[64];
+	int top = 0;
+	int hit = -1;
+	int node = 0;
+	for (int step = 0; step < (1 << 24); ++step)
+	{
+		V4 node0 = b.row(node * 2);
+		V4 node1 = b.row(node * 2 + 1);
+		if (node1.w >= 0.0f)
+		{
+			int first = int(node0.w);
+			int count = int(node1.w);
+			for (int t = first; t < first + count; ++t)
+			{
+				float h = intersectTriangle(o, d, b.vertex(t, 0), b.vertex(t, 1), b.vertex(t, 2));
+				if (h > 0.0f && (h < distance || (h == distance && hit >= 0 && t < hit)) && accept(t))
+				{
+					distance = h;
+					hit = t;
+				}
+			}
+		}
+		else
+		{
+			int left = node + 1;
+			int right = int(node0.w);
+			float leftDistance = intersectBox(o, inv, b.row(left * 2).xyz(), b.row(left * 2 + 1).xyz(), distance);
+			float rightDistance = intersectBox(o, inv, b.row(right * 2).xyz(), b.row(right * 2 + 1).xyz(), distance);
+			bool visitLeft = leftDistance >= 0.0f;
+			bool visitRight = rightDistance >= 0.0f;
+			if (visitLeft && visitRight)
+			{
+				bool leftFirst = leftDistance <= rightDistance;
+				if (top < 64)
+				{
+					stack[top++] = leftFirst ? right : left;
+				}
+				else
+				{
+					raiseStatus(1u);
+				}
+				node = leftFirst ? left : right;
+				continue;
+			}
+			if (visitLeft || visitRight)
+			{
+				node = visitLeft ? left : right;
+				continue;
+			}
+		}
+		// Pop, skipping subtrees that the nearest hit found since rules out.
+		bool found = false;
+		while (top > 0)
+		{
+			int candidate = stack[--top];
+			if (intersectBox(o, inv, b.row(candidate * 2).xyz(), b.row(candidate * 2 + 1).xyz(), distance) >= 0.0f)
+			{
+				node = candidate;
+				found = true;
+				break;
+			}
+		}
+		if (!found)
+		{
+			break;
+		}
+	}
+	return hit;
+}
+
+} // namespace restir

@@ -1,0 +1,71 @@
+// restir_trace: a fixed ray set through the BVH (bvh.sh:298-319), one thread
+// per ray. Closest-hit rays keep their short stack in shared memory,
+// interleaved so that the 32 lanes of a warp touch 32 different banks.
+#include "bvh.cuh"
+#include "watertight.cuh"
+
+namespace restir
+{
+namespace
+{
+
+constexpr int kTraceBlock = 128;
+
+__global__ void __launch_bounds__(kTraceBlock) traceKernel(BvhView bvh, const float4* __restrict__ rays,
+	int32_t* __restrict__ hitTriangle, float* __restrict__ hitDistance, uint32_t n, int kind)
+{
+	__shared__ int stack[kBvhShortStack * kTraceBlock];
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n)
+	{
+		return;
+	}
+	float4 a = __ldg(rays + 2 * i);
+	float4 b = __ldg(rays + 2 * i + 1);
+	V3 o = v3(a.x, a.y, a.z);
+	V3 d = v3(b.x, b.y, b.z);
+	float distance = a.w;
+	int hit = -1;
+	if (kind == RESTIR_TRACE_CLOSEST)
+	{
+		hit = traceBvh(bvh, o, d, a.w, false, distance, stack + threadIdx.x, kTraceBlock);
+	}
+	else if (kind == RESTIR_TRACE_ANY)
+	{
+		hit = traceBvh(bvh, o, d, a.w, true, distance, nullptr, 0);
+	}
+	else if (kind == RESTIR_TRACE_CLOSEST_STACKLESS)
+	{
+		hit = traceBvh(bvh, o, d, a.w, false, distance, nullptr, 0);
+	}
+	else
+	{
+		hit = traceWatertight(bvh, o, d, distance);
+	}
+	hitTriangle[i] = hit;
+	hitDistance[i] = distance;
+}
+
+} // namespace
+} // namespace restir
+
+using namespace restir;
+
+extern "C" int restir_trace(const RestirParams* params, const RestirScene* scene, const float* rays,
+	int32_t* hit_triangle, float* hit_distance, uint32_t n, int kind, void* stream)
+{
+	(void)params;
+	if (scene == nullptr || rays == nullptr || hit_triangle == nullptr || hit_distance == nullptr
+		|| kind < RESTIR_TRACE_CLOSEST || kind > RESTIR_TRACE_CLOSEST_WATERTIGHT)
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	if (n == 0u)
+	{
+		return RESTIR_OK;
+	}
+	BvhView bvh = makeBvhView(scene);
+	traceKernel<<<(n + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, asStream(stream)>>>(
+		bvh, reinterpret_cast<const float4*>(rays), hit_triangle, hit_distance, n, kind);
+	return launchStatus();
+}

@@ -1,0 +1,172 @@
+// Watertight ray/triangle intersection (Woop, Benthin and Wald, "Watertight
+// Ray/Triangle Intersection", JCGT 2(1), 2013): the ray is sheared so that
+// it runs along +z, the three edge functions are evaluated in the sheared
+// 2D plane (in double precision when one of them is exactly zero), and a hit
+// on an edge shared by two triangles is reported by at least one of them.
+// The production alternative to the reference's Moeller-Trumbore test
+// (bvh.sh:44-71), whose rays can slip through shared edges.
+#pragma once
+
+#include "bvh.cuh"
+
+namespace restir
+{
+
+struct WatertightRay
+{
+	int kx, ky, kz;
+	float sx, sy, sz;
+	V3 o;
+};
+
+__device__ __forceinline__ float component(V3 v, int k)
+{
+	return k == 0 ? v.x : (k == 1 ? v.y : v.z);
+}
+
+__device__ __forceinline__ WatertightRay makeWatertightRay(V3 o, V3 d)
+{
+	WatertightRay r;
+	V3 a = vabs(d);
+	int kz = a.x > a.y ? (a.x > a.z ? 0 : 2) : (a.y > a.z ? 1 : 2);
+	int kx = kz + 1 == 3 ? 0 : kz + 1;
+	int ky = kx + 1 == 3 ? 0 : kx + 1;
+	if (component(d, kz) < 0.0f)
+	{
+		int t = kx;
+		kx = ky;
+		ky = t;
+	}
+	r.kx = kx;
+	r.ky = ky;
+	r.kz = kz;
+	r.sx = component(d, kx) / component(d, kz);
+	r.sy = component(d, ky) / component(d, kz);
+	r.sz = 1.0f / component(d, kz);
+	r.o = o;
+	return r;
+}
+
+// Distance to the triangle, or -1; hits must lie in (0, tmax].
+__device__ __forceinline__ float intersectWatertight(const WatertightRay& r, V3 v0, V3 v1, V3 v2, float tmax)
+{
+	V3 A = v0 - r.o;
+	V3 B = v1 - r.o;
+	V3 C = v2 - r.o;
+	float az = component(A, r.kz), bz = component(B, r.kz), cz = component(C, r.kz);
+	float ax = component(A, r.kx) - r.sx * az;
+	float ay = component(A, r.ky) - r.sy * az;
+	float bx = component(B, r.kx) - r.sx * bz;
+	float by = component(B, r.ky) - r.sy * bz;
+	float cx = component(C, r.kx) - r.sx * cz;
+	float cy = component(C, r.ky) - r.sy * cz;
+	float u = cx * by - cy * bx;
+	float v = ax * cy - ay * cx;
+	float w = bx * ay - by * ax;
+	if (u == 0.0f || v == 0.0f || w == 0.0f)
+	{
+		u = float(double(cx) * double(by) - double(cy) * double(bx));
+		v = float(double(ax) * double(cy) - double(ay) * double(cx));
+		w = float(double(bx) * double(ay) - double(by) * double(ax));
+	}
+	if ((u < 0.0f || v < 0.0f || w < 0.0f) && (u > 0.0f || v > 0.0f || w > 0.0f))
+	{
+		return -1.0f;
+	}
+	float det = u + v + w;
+	if (det == 0.0f)
+	{
+		return -1.0f;
+	}
+	float sz = r.sz;
+	float t = u * (sz * az) + v * (sz * bz) + w * (sz * cz);
+	float sign = det < 0.0f ? -1.0f : 1.0f;
+	float signedT = t * sign;
+	float absDet = det * sign;
+	if (signedT <= 0.0f || signedT > tmax * absDet)
+	{
+		return -1.0f;
+	}
+	return t / det;
+}
+
+// Nearest watertight hit in (0, distance], ties to the lower triangle index;
+// full stack, nearest child first.
+__device__ inline int traceWatertight(const BvhView& b, V3 o, V3 d, float& distance)
+{
+	WatertightRay ray = makeWatertightRay(o, d);
+	V3 inv = bvhInverseDirection(d);
+	if (!b.available() || intersectBox(o, inv, b.row(0).xyz(), b.row(1).xyz(), distance) < 0.0f)
+	{
+		return -1;
+	}
+	int stack[64];
+	int top = 0;
+	int hit = -1;
+	int node = 0;
+	for (int step = 0; step < (1 << 24); ++step)
+	{
+		V4 node0 = b.row(node * 2);
+		V4 node1 = b.row(node * 2 + 1);
+		if (node1.w >= 0.0f)
+		{
+			int first = int(node0.w);
+			int count = int(node1.w);
+			for (int t = first; t < first + count; ++t)
+			{
+				float h = intersectWatertight(ray, b.vertex(t, 0), b.vertex(t, 1), b.vertex(t, 2), distance);
+				if (h > 0.0f && (h < distance || (h == distance && (hit < 0 || t < hit))))
+				{
+					distance = h;
+					hit = t;
+				}
+			}
+		}
+		else
+		{
+			int left = node + 1;
+			int right = int(node0.w);
+			float leftDistance = intersectBox(o, inv, b.row(left * 2).xyz(), b.row(left * 2 + 1).xyz(), distance);
+			float rightDistance = intersectBox(o, inv, b.row(right * 2).xyz(), b.row(right * 2 + 1).xyz(), distance);
+			bool visitLeft = leftDistance >= 0.0f;
+			bool visitRight = rightDistance >= 0.0f;
+			if (visitLeft && visitRight)
+			{
+				bool leftFirst = leftDistance <= rightDistance;
+				if (top < 64)
+				{
+					stack[top++] = leftFirst ? right : left;
+				}
+				else
+				{
+					raiseStatus(1u);
+				}
+				node = leftFirst ? left : right;
+				continue;
+			}
+			if (visitLeft || visitRight)
+			{
+				node = visitLeft ? left : right;
+				continue;
+			}
+		}
+		bool found = false;
+		while (top > 0)
+		{
+			int candidate = stack[--top];
+			if (intersectBox(o, inv, b.row(candidate * 2).xyz(), b.row(candidate * 2 + 1).xyz(), distance) >= 0.0f)
+			{
+				node = candidate;
+				found = true;
+				break;
+			}
+		}
+		if (!found)
+		{
+			break;
+		}
+	}
+	return hit;
+}
+
+} // namespace restir
