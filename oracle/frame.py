@@ -1,0 +1,237 @@
+"""ORACLE (test infrastructure): the reference's per-frame pass sequence
+(src/renderer.cpp:435-1125) over either backend, for parity tests and the
+CPU baseline.
+
+FrameRunner owns one frame's buffers and history with the reference's
+ping-pong (renderer.h:218-219, renderer.cpp:706, 1122) and runs the passes in
+the reference's order. backend="oracle" calls oracle/liboracle.so on numpy
+arrays; backend="cuda" calls restir_b200's C ABI on torch tensors on cuda:0.
+In check mode (run_checked) every CUDA pass is fed the oracle's inputs and
+its outputs are compared with the oracle's bit for bit, pass by pass.
+
+The frame uniforms come from the library's own host code
+(restir_frame_params), which is host logic, not a pass.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+import restir_b200 as rb
+from restir_b200.abi import RestirDiReservoirs, RestirGBuffer, RestirGiHistory, RestirGiReservoirs
+
+from . import binding as ob
+
+# name: (dtype, channels, resolution) with resolution "full", "gi", "atlas", "grid", "none"
+LAYOUT = {
+    "gb.albedo": (np.uint8, 4, "full"), "gb.normal": (np.uint8, 4, "full"), "gb.emissive": (np.uint16, 4, "full"),
+    "gb.shading_normal": (np.uint8, 4, "full"), "gb.depth": (np.float32, 1, "full"),
+    "atlas": (np.float32, 1, "atlas"),
+    "di.sample0": (np.float32, 4, "full"), "di.receiver0": (np.float32, 4, "full"), "di.normal0": (np.uint16, 4, "full"),
+    "di.sample1": (np.float32, 4, "full"), "di.receiver1": (np.float32, 4, "full"), "di.normal1": (np.uint16, 4, "full"),
+    "di.diffuse": (np.uint16, 4, "full"), "di.specular": (np.uint16, 4, "full"), "black": (np.uint16, 4, "full"),
+    "grid0": (np.uint32, 1, "grid"), "grid1": (np.uint32, 1, "grid"),
+    "gi.sample0": (np.float32, 4, "gi"), "gi.receiver0": (np.float32, 4, "gi"), "gi.normal0": (np.float32, 4, "gi"),
+    "gi.sample1": (np.float32, 4, "gi"), "gi.receiver1": (np.float32, 4, "gi"), "gi.normal1": (np.float32, 4, "gi"),
+    "gi.color0": (np.uint16, 4, "gi"), "gi.color1": (np.uint16, 4, "gi"),
+    "gi.moments0": (np.uint16, 4, "gi"), "gi.moments1": (np.uint16, 4, "gi"),
+    "filtered0": (np.uint16, 4, "gi"), "filtered1": (np.uint16, 4, "gi"),
+    "filter0": (np.uint16, 4, "gi"), "filter1": (np.uint16, 4, "gi"),
+    "hdr": (np.uint16, 4, "full"),
+    "ref.mean": (np.float64, 3, "full"), "ref.alpha": (np.uint8, 1, "full"),
+}
+
+
+class FrameRunner:
+    def __init__(self, setup, width: int, height: int, backend: str = "oracle", settings=None):
+        self.setup = setup
+        self.backend = backend
+        self.settings = settings or setup.settings
+        self.width, self.height = width, height
+        self.state = rb.initial_state()
+        self.history_read = 0
+        self.di_read = 0
+        self.params = None
+        self.plan = None
+        self.frame_input = rb.frame_input(setup.mesh, width, height)
+        p, _ = rb.frame_params(self.settings, setup.mesh, setup.lights.count, setup.bvh, self.frame_input, self.state)
+        self.shape = {"full": width * height, "gi": p.gi_width * p.gi_height,
+                      "atlas": 6 * p.shadow_face_size * p.shadow_face_size,
+                      "grid": p.grid_table_size * (2 + p.grid_cell_capacity)}
+        self.buffers = {}
+        for name, (dt, ch, res) in LAYOUT.items():
+            n = self.shape[res] * ch
+            self.buffers[name] = np.zeros(n, dt)
+        if backend == "cuda":
+            import torch
+            self.buffers = {k: torch.from_numpy(v).cuda() for k, v in self.buffers.items()}
+            self.scene = setup.device_scene()
+            self.lib = rb.load()
+        else:
+            self.scene = setup.host_scene()
+            self.lib = ob.load()
+        self.error_scratch = None
+
+    # --- pass plumbing --------------------------------------------------------------------------------
+
+    def b(self, name):
+        return rb.ptr(self.buffers[name])
+
+    def gbuffer(self) -> RestirGBuffer:
+        g = RestirGBuffer()
+        for f in ("albedo", "normal", "emissive", "shading_normal", "depth"):
+            setattr(g, f, self.b("gb." + f))
+        return g
+
+    def call(self, name, *args):
+        if self.backend == "cuda":
+            rb.check(getattr(self.lib, "restir_" + name)(*args, None), name)
+        else:
+            rb.check(getattr(self.lib, "oracle_" + name)(*args), name)
+
+    def prepare(self):
+        self.params, self.plan = rb.frame_params(self.settings, self.setup.mesh, self.setup.lights.count,
+                                                 self.setup.bvh, self.frame_input, self.state)
+        return self.params, self.plan
+
+    # --- the frame ------------------------------------------------------------------------------------
+
+    def passes(self):
+        """The frame as (pass name, callable) in the reference's order."""
+        P, plan = self.params, self.plan
+        hw = 1 - self.history_read
+        hr = self.history_read
+        dw = 1 - self.di_read
+        gb = self.gbuffer()
+        out = []
+        out.append(("shadow_atlas", lambda: self.call("shadow_atlas", P, self.scene, self.b("atlas"))))
+        out.append(("gbuffer_primary", lambda: self.call("gbuffer_primary", P, self.scene, gb)))
+        if plan.di_active:
+            prev = RestirDiReservoirs(self.b(f"di.sample{self.di_read}"), self.b(f"di.receiver{self.di_read}"),
+                                      self.b(f"di.normal{self.di_read}"))
+            cur = RestirDiReservoirs(self.b(f"di.sample{dw}"), self.b(f"di.receiver{dw}"), self.b(f"di.normal{dw}"))
+            out.append(("di_temporal", lambda: self.call("di_temporal", P, self.scene, gb, prev, cur)))
+            out.append(("di_spatial", lambda: self.call("di_spatial", P, self.scene, gb, cur, self.b("di.diffuse"),
+                                                       self.b("di.specular"))))
+        if plan.surface_light_is_di:
+            surface = self.b("di.diffuse") if plan.di_active else self.b("black")
+        else:
+            surface = self.b("gb.emissive")
+        out.append(("grid_clear", lambda: self.call("grid_clear", P, self.b(f"grid{hw}"))))
+        out.append(("grid_insert", lambda: self.call("grid_insert", P, gb, self.b(f"grid{hw}"))))
+        color_read = self.b(f"filtered{hr}") if plan.denoiser else self.b(f"gi.color{hr}")
+        history = RestirGiHistory(self.b(f"gi.sample{hr}"), self.b(f"gi.receiver{hr}"), self.b(f"gi.normal{hr}"),
+                                  color_read, self.b(f"gi.moments{hr}"))
+        current = RestirGiReservoirs(self.b(f"gi.sample{hw}"), self.b(f"gi.receiver{hw}"), self.b(f"gi.normal{hw}"))
+        out.append(("gi_temporal", lambda: self.call("gi_temporal", P, self.scene, gb, history, self.b(f"grid{hr}"),
+                                                     self.b("atlas"), surface, current)))
+        out.append(("gi_spatial", lambda: self.call("gi_spatial", P, self.scene, gb, current, self.b(f"grid{hw}"),
+                                                    history, self.b("atlas"), surface, self.b(f"gi.color{hw}"),
+                                                    self.b(f"gi.moments{hw}"))))
+        denoised = f"gi.color{hw}"
+        if plan.denoiser:
+            out.append(("svgf_variance", lambda: self.call("svgf_variance", P, self.b(f"gi.color{hw}"),
+                                                           self.b(f"gi.moments{hw}"), self.b(f"gi.receiver{hw}"),
+                                                           self.b(f"gi.normal{hw}"), self.b("filter0"))))
+            for it in range(plan.atrous_iterations):
+                src = "filter0" if it == 0 else (f"filtered{hw}" if it == 1 else f"filter{(it - 1) & 1}")
+                dst = f"filtered{hw}" if it == 0 else f"filter{it & 1}"
+                denoised = dst
+                out.append((f"svgf_atrous{it}", (lambda s=src, d=dst, step=1 << it: self.call(
+                    "svgf_atrous", P, step, self.b(s), self.b(f"gi.receiver{hw}"), self.b(f"gi.normal{hw}"),
+                    self.b(d)))))
+        di_d = self.b("di.diffuse") if plan.di_active else self.b("black")
+        di_s = self.b("di.specular") if plan.di_active else self.b("black")
+        out.append(("composite", lambda: self.call("composite", P, gb, self.b("atlas"), self.b(denoised), di_d, di_s,
+                                                   self.b("hdr"))))
+        if plan.reference_accumulate:
+            out.append(("reference_accumulate", lambda: self.call(
+                "reference_accumulate", P, self.b("hdr"), self.b("ref.mean"), self.b("ref.alpha"),
+                plan.reference_weight_frames)))
+        return out
+
+    def finish(self):
+        rb.advance(self.params, self.plan, self.frame_input, self.state)
+        self.history_read = 1 - self.history_read
+        if self.plan.di_active:
+            self.di_read = 1 - self.di_read
+
+    def render(self):
+        self.prepare()
+        for _, fn in self.passes():
+            fn()
+        if self.backend == "cuda":
+            import torch
+            torch.cuda.synchronize()
+        self.finish()
+
+    def set_reference_accumulation(self, accumulate: bool):
+        """Renderer::setReferenceAccumulation (renderer.cpp:1128-1141)."""
+        if bool(self.state.reference_accumulating) == accumulate:
+            return
+        self.state.reference_accumulating = int(accumulate)
+        if accumulate:
+            self.state.reference_frames = 0
+        self.state.history_valid = 0
+
+    def error(self) -> np.ndarray:
+        """cs_error.sc against the reference, FP64: relMSE, mean image, mean reference, count."""
+        P = self.params
+        out = np.zeros(4, np.float64)
+        if self.backend == "cuda":
+            import torch
+            if self.error_scratch is None:
+                nbytes = self.lib.restir_error_scratch_bytes(self.width, self.height)
+                self.error_scratch = torch.zeros(nbytes // 8 + 1, dtype=torch.float64, device="cuda")
+            d = torch.zeros(4, dtype=torch.float64, device="cuda")
+            rb.check(self.lib.restir_error(P, self.b("hdr"), self.b("ref.mean"), self.b("ref.alpha"), d.data_ptr(),
+                                           self.error_scratch.data_ptr(), None), "error")
+            out[:] = d.cpu().numpy()
+        else:
+            rb.check(self.lib.oracle_error(P, self.b("hdr"), self.b("ref.mean"), self.b("ref.alpha"),
+                                           out.ctypes.data), "error")
+        return out
+
+    def host(self, name) -> np.ndarray:
+        v = self.buffers[name]
+        return v.cpu().numpy() if hasattr(v, "cpu") else v
+
+
+def run_checked(setup, width: int, height: int, frames: int, settings=None, on_mismatch=None,
+                reference_frames: int = 0):
+    """Runs `frames` frames on both backends, feeding each CUDA pass the oracle's
+    inputs and comparing its outputs bit for bit. Returns {pass: mismatching elements}."""
+    import torch
+    oracle_run = FrameRunner(setup, width, height, "oracle", settings)
+    cuda_run = FrameRunner(setup, width, height, "cuda", settings)
+    report = {}
+    for frame in range(frames):
+        if reference_frames and frame == frames - reference_frames:
+            oracle_run.set_reference_accumulation(True)
+            cuda_run.set_reference_accumulation(True)
+        oracle_run.prepare()
+        cuda_run.prepare()
+        for (name, o_fn), (_, c_fn) in zip(oracle_run.passes(), cuda_run.passes()):
+            before = {k: v.copy() for k, v in oracle_run.buffers.items()}
+            o_fn()
+            changed = [k for k in before if not np.array_equal(before[k], oracle_run.buffers[k])]
+            # The CUDA pass gets exactly the oracle's inputs.
+            for k, v in before.items():
+                cuda_run.buffers[k].copy_(torch.from_numpy(v))
+            c_fn()
+            torch.cuda.synchronize()
+            for k in changed + [k for k in before if k not in changed and name.startswith("grid")]:
+                got = cuda_run.host(k)
+                want = oracle_run.buffers[k]
+                if k.startswith("grid"):
+                    continue  # compared cell by cell in test_grid_gpu
+                bad = int(np.count_nonzero(got.view(np.uint8) != want.view(np.uint8)))
+                if bad:
+                    report[f"{frame}:{name}:{k}"] = bad
+                    if on_mismatch:
+                        on_mismatch(frame, name, k, got, want)
+            # Continue from the oracle's state for the grid (its slot order is scheduling-dependent).
+        oracle_run.finish()
+        cuda_run.finish()
+    return report, oracle_run, cuda_run

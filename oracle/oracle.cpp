@@ -161,44 +161,14 @@ const int threadCount = threads();
 namespace
 {
 
-/* Nearest hit with t in (0, tmax) among the triangles _accept lets through,
- * ties to the lower triangle index (order independent). */
+/* Moeller-Trumbore nearest hit in (0, tmax) among the triangles _accept
+ * lets through (the raster passes' ray casts). */
 template<typename Accept>
 int traceNearestFiltered(const Bvh& b, vec3 _origin, vec3 _direction, float& _distance, Accept _accept)
 {
-	vec3 inverseDirection = bvhInverseDirection(_direction);
-	int hit = -1;
-	int node = 0;
-	for (int step = 0; step < 1 << 24; ++step)
-	{
-		if (node >= b.nodeCount)
-		{
-			break;
-		}
-		vec4 node0 = b.row(node * 2);
-		vec4 node1 = b.row(node * 2 + 1);
-		bool leaf = node1.w >= 0.0f;
-		if (intersectBox(_origin, inverseDirection, node0.xyz(), node1.xyz(), _distance) < 0.0f)
-		{
-			node = leaf ? node + 1 : int(-node1.w) - 1;
-			continue;
-		}
-		if (leaf)
-		{
-			int first = int(node0.w), count = int(node1.w);
-			for (int t = first; t < first + count; ++t)
-			{
-				float d = intersectTriangle(_origin, _direction, b.vertex(t, 0), b.vertex(t, 1), b.vertex(t, 2));
-				if (d > 0.0f && (d < _distance || (d == _distance && hit >= 0 && t < hit)) && _accept(t))
-				{
-					_distance = d;
-					hit = t;
-				}
-			}
-		}
-		node = node + 1;
-	}
-	return hit;
+	return traceNearestFirst(b, _origin, _direction, _distance, false,
+		[&](int t, float) { return intersectTriangle(_origin, _direction, b.vertex(t, 0), b.vertex(t, 1), b.vertex(t, 2)); },
+		_accept);
 }
 
 vec3 clipToWorld(const mat4& _inverse, vec3 _clip)

@@ -407,38 +407,100 @@ inline float intersectWatertight(vec3 _origin, vec3 _direction, vec3 _v0, vec3 _
 	return t / det;
 }
 
-/* Nearest watertight hit, ties to the lower triangle index, stackless walk. */
-inline int traceWatertight(const Bvh& b, vec3 _origin, vec3 _direction, float& _distance)
+/* Nearest hit in (0, distance) among the triangles _accept lets through,
+ * ties to the lower triangle index, nearest child first with a full stack
+ * (the order of the kernels' traversal, so that box culling decides alike).
+ * _test(t, distance) is the triangle test; _conservative widens each box's
+ * exit distance by 1 + 2 gamma_3 (Ize, "Robust BVH Ray Traversal", JCGT
+ * 2(2), 2013) for the watertight mode. */
+template<typename Test, typename Accept>
+int traceNearestFirst(const Bvh& b, vec3 _origin, vec3 _direction, float& _distance, bool _conservative, Test _test,
+	Accept _accept)
 {
-	vec3 inverseDirection = bvhInverseDirection(_direction);
+	vec3 inv = bvhInverseDirection(_direction);
+	const float widen = _conservative ? 1.00000036f : 1.0f;
+	auto box = [&](int node) -> float
+	{
+		vec3 t0 = (b.row(node * 2).xyz() - _origin) * inv;
+		vec3 t1 = (b.row(node * 2 + 1).xyz() - _origin) * inv;
+		vec3 n = min(t0, t1);
+		vec3 f = max(t0, t1);
+		float enter = max(max(n.x, n.y), max(n.z, 0.0f));
+		float leave = min(min(f.x, f.y), f.z) * widen;
+		leave = min(leave, _distance);
+		return enter <= leave ? enter : -1.0f;
+	};
+	if (!b.available() || box(0) < 0.0f)
+	{
+		return -1;
+	}
+	std::vector<int> stack;
 	int hit = -1;
 	int node = 0;
-	while (node < b.nodeCount)
+	for (;;)
 	{
 		vec4 node0 = b.row(node * 2);
 		vec4 node1 = b.row(node * 2 + 1);
-		bool leaf = node1.w >= 0.0f;
-		if (intersectBox(_origin, inverseDirection, node0.xyz(), node1.xyz(), _distance) < 0.0f)
-		{
-			node = leaf ? node + 1 : int(-node1.w) - 1;
-			continue;
-		}
-		if (leaf)
+		if (node1.w >= 0.0f)
 		{
 			int first = int(node0.w), count = int(node1.w);
 			for (int t = first; t < first + count; ++t)
 			{
-				float d = intersectWatertight(_origin, _direction, b.vertex(t, 0), b.vertex(t, 1), b.vertex(t, 2), _distance);
-				if (d > 0.0f && (d < _distance || (d == _distance && (hit < 0 || t < hit))))
+				float h = _test(t, _distance);
+				if (h > 0.0f && (h < _distance || (h == _distance && hit >= 0 && t < hit)) && _accept(t))
 				{
-					_distance = d;
+					_distance = h;
 					hit = t;
 				}
 			}
 		}
-		node = node + 1;
+		else
+		{
+			int left = node + 1;
+			int right = int(node0.w);
+			float leftDistance = box(left);
+			float rightDistance = box(right);
+			bool visitLeft = leftDistance >= 0.0f;
+			bool visitRight = rightDistance >= 0.0f;
+			if (visitLeft && visitRight)
+			{
+				bool leftFirst = leftDistance <= rightDistance;
+				stack.push_back(leftFirst ? right : left);
+				node = leftFirst ? left : right;
+				continue;
+			}
+			if (visitLeft || visitRight)
+			{
+				node = visitLeft ? left : right;
+				continue;
+			}
+		}
+		bool found = false;
+		while (!stack.empty())
+		{
+			int candidate = stack.back();
+			stack.pop_back();
+			if (box(candidate) >= 0.0f)
+			{
+				node = candidate;
+				found = true;
+				break;
+			}
+		}
+		if (!found)
+		{
+			break;
+		}
 	}
 	return hit;
+}
+
+/* Nearest watertight hit, ties to the lower triangle index. */
+inline int traceWatertight(const Bvh& b, vec3 _origin, vec3 _direction, float& _distance)
+{
+	return traceNearestFirst(b, _origin, _direction, _distance, true,
+		[&](int t, float tmax) { return intersectWatertight(_origin, _direction, b.vertex(t, 0), b.vertex(t, 1), b.vertex(t, 2), tmax); },
+		[](int) { return true; });
 }
 
 inline vec3 bvhTriangleAlbedo(const Bvh& b, int _triangle)

@@ -244,14 +244,31 @@ __device__ __forceinline__ int traceBvh(const BvhView& b, V3 o, V3 d, float maxD
 }
 
 // Nearest hit in (0, distance) among the triangles accept() lets through,
-// ties to the lower triangle index, so the result does not depend on the
-// visiting order. A full stack of 64 entries in local memory, nearest child
-// first; the layout's depth is at most 40 (bvh.h:49), so it cannot overflow.
-template<typename Accept>
-__device__ inline int traceNearestFiltered(const BvhView& b, V3 o, V3 d, float& distance, Accept accept)
+// ties to the lower triangle index, nearest child first with a full stack of
+// 64 entries in local memory (the layout's depth is at most 40, bvh.h:49).
+// test(t, distance) is the triangle test. With conservative set, a box's exit
+// distance is widened by 1 + 2 gamma_3 (Ize, "Robust BVH Ray Traversal",
+// JCGT 2(2), 2013), so that rounding in the slab test never culls a box
+// whose triangle the watertight test hits.
+template<typename Test, typename Accept>
+__device__ inline int traceNearestFirst(const BvhView& b, V3 o, V3 d, float& distance, bool conservative, Test test, Accept accept)
 {
 	V3 inv = bvhInverseDirection(d);
-	if (!b.available() || intersectBox(o, inv, b.row(0).xyz(), b.row(1).xyz(), distance) < 0.0f)
+	const float widen = conservative ? 1.00000036f : 1.0f;
+	auto box = [&](int node) -> float
+	{
+		V3 lo = b.row(node * 2).xyz();
+		V3 hi = b.row(node * 2 + 1).xyz();
+		V3 t0 = (lo - o) * inv;
+		V3 t1 = (hi - o) * inv;
+		V3 n = vmin(t0, t1);
+		V3 f = vmax(t0, t1);
+		float enter = fmaxf(fmaxf(n.x, n.y), fmaxf(n.z, 0.0f));
+		float leave = fminf(fminf(f.x, f.y), f.z) * widen;
+		leave = fminf(leave, distance);
+		return enter <= leave ? enter : -1.0f;
+	};
+	if (!b.available() || box(0) < 0.0f)
 	{
 		return -1;
 	}
@@ -269,7 +286,7 @@ __device__ inline int traceNearestFiltered(const BvhView& b, V3 o, V3 d, float& 
 			int count = int(node1.w);
 			for (int t = first; t < first + count; ++t)
 			{
-				float h = intersectTriangle(o, d, b.vertex(t, 0), b.vertex(t, 1), b.vertex(t, 2));
+				float h = test(t, distance);
 				if (h > 0.0f && (h < distance || (h == distance && hit >= 0 && t < hit)) && accept(t))
 				{
 					distance = h;
@@ -281,8 +298,8 @@ __device__ inline int traceNearestFiltered(const BvhView& b, V3 o, V3 d, float& 
 		{
 			int left = node + 1;
 			int right = int(node0.w);
-			float leftDistance = intersectBox(o, inv, b.row(left * 2).xyz(), b.row(left * 2 + 1).xyz(), distance);
-			float rightDistance = intersectBox(o, inv, b.row(right * 2).xyz(), b.row(right * 2 + 1).xyz(), distance);
+			float leftDistance = box(left);
+			float rightDistance = box(right);
 			bool visitLeft = leftDistance >= 0.0f;
 			bool visitRight = rightDistance >= 0.0f;
 			if (visitLeft && visitRight)
@@ -310,7 +327,7 @@ __device__ inline int traceNearestFiltered(const BvhView& b, V3 o, V3 d, float& 
 		while (top > 0)
 		{
 			int candidate = stack[--top];
-			if (intersectBox(o, inv, b.row(candidate * 2).xyz(), b.row(candidate * 2 + 1).xyz(), distance) >= 0.0f)
+			if (box(candidate) >= 0.0f)
 			{
 				node = candidate;
 				found = true;
@@ -323,6 +340,15 @@ __device__ inline int traceNearestFiltered(const BvhView& b, V3 o, V3 d, float& 
 		}
 	}
 	return hit;
+}
+
+// Moeller-Trumbore nearest hit among accepted triangles (the raster
+// passes' ray casts).
+template<typename Accept>
+__device__ inline int traceNearestFiltered(const BvhView& b, V3 o, V3 d, float& distance, Accept accept)
+{
+	return traceNearestFirst(b, o, d, distance, false,
+		[&](int t, float) { return intersectTriangle(o, d, b.vertex(t, 0), b.vertex(t, 1), b.vertex(t, 2)); }, accept);
 }
 
 } // namespace restir

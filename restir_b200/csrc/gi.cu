@@ -1,0 +1,485 @@
+// ReSTIR GI passes: restir_gi_temporal (cs_restir_temporal.sc:57-297) and
+// restir_gi_spatial (cs_restir_spatial.sc:49-246).
+//
+// The temporal pass runs one warp per 4x8 pixel group of the reference
+// (compute.sh:31-35): the boiling filter's tile mean is a warp-shuffle tree
+// in the order of the shader's shared-memory reduction (compute.sh:375-386),
+// and closest-hit candidate rays keep their short traversal stack in shared
+// memory, interleaved across the block's lanes.
+#include "gi.cuh"
+
+namespace restir
+{
+namespace
+{
+
+constexpr int kGiWarps = 4;
+constexpr int kGiThreads = 32 * kGiWarps;
+
+struct GiBindings
+{
+	const uint8_t* albedo;
+	const uint8_t* normal;
+	const float* depth;
+	const float4* historySample;
+	const float4* historyReceiver;
+	const float4* historyNormal;
+	const uint16_t* historyColor;
+	const uint16_t* historyMoments;
+	const uint16_t* surfaceLight;
+	const float* shadowAtlas;
+	const uint32_t* grid;
+	const float4* reservoirSample;   // spatial: this frame's reservoirs
+	const float4* reservoirReceiver;
+	const float4* reservoirNormal;
+	float4* outSample;               // temporal outputs
+	float4* outReceiver;
+	float4* outNormal;
+	uint16_t* outColor;              // spatial outputs
+	uint16_t* outMoments;
+};
+
+__device__ __forceinline__ GiPass makePass(const RestirParams& P, const BvhView& bvh, const GiBindings& b, const float* gridCamera,
+	int* stack, int stride)
+{
+	GiPass g{ P };
+	g.bvh = bvh;
+	g.grid = makeGridView(&P, b.grid, gridCamera);
+	g.albedoTex = b.albedo;
+	g.normalTex = b.normal;
+	g.depthTex = b.depth;
+	g.historyNormal = b.historyNormal;
+	g.historyReceiver = b.historyReceiver;
+	g.historyColor = b.historyColor;
+	g.surfaceLight = b.surfaceLight;
+	g.shadowAtlas = b.shadowAtlas;
+	g.stack = stack;
+	g.stackStride = stride;
+	g.W = int(P.width);
+	g.H = int(P.height);
+	g.w = int(P.gi_width);
+	g.h = int(P.gi_height);
+	g.giSize = v2(float(g.w), float(g.h));
+	g.giTexel = v2(1.0f / float(g.w), 1.0f / float(g.h));
+	return g;
+}
+
+__device__ __forceinline__ V4 f4(float4 q)
+{
+	return { q.x, q.y, q.z, q.w };
+}
+
+__global__ void __launch_bounds__(kGiThreads) giTemporalKernel(const RestirParams P, BvhView bvh, GiBindings b)
+{
+	__shared__ int stackStorage[kBvhShortStack * kGiThreads];
+	const int lane = int(threadIdx.x & 31u);
+	const int groupsX = (int(P.gi_width) + 3) / 4;
+	const int groupsY = (int(P.gi_height) + 7) / 8;
+	const int group = int(blockIdx.x) * kGiWarps + int(threadIdx.x >> 5);
+	if (group >= groupsX * groupsY)
+	{
+		return; // whole warp
+	}
+	GiPass g = makePass(P, bvh, b, P.prev_camera_position, stackStorage + threadIdx.x, kGiThreads);
+	const int px = (group % groupsX) * 4 + (lane & 3);
+	const int py = (group / groupsX) * 8 + (lane >> 2);
+	const bool inside = px < g.w && py < g.h;
+	const V2 uv = pixelUv(px, py, g.giTexel);
+	const float depth = inside ? g.depthAt(uv) : 1.0f;
+	const bool working = inside && depth < kSkyDepth;
+
+	const V3 position = reconstructWorldPosition(P, uv, depth);
+	const V3 normal = g.decode(uv);
+	const V3 albedo = g.diffuseAlbedo(uv);
+	const V3 rayOrigin = position + normal * g.kRayBias();
+	const V2 giPixelCoord = v2(floorf(uv.x * g.giSize.x), floorf(uv.y * g.giSize.y));
+	uint32_t rng = pcg(uint32_t(giPixelCoord.x) + pcg(uint32_t(giPixelCoord.y) + pcg(uint32_t(P.frame_index))));
+
+	GiReservoir canonical = emptyReservoir();
+	for (int sampleIndex = 0; sampleIndex < P.initial_candidates; ++sampleIndex)
+	{
+		float random0 = nextRandom(rng);
+		float random1 = nextRandom(rng);
+		float randomSelect = nextRandom(rng);
+		V3 direction = GiPass::cosineHemisphere(normal, random0, random1);
+		canonical.count += 1.0f;
+		V3 hitPosition = v3s(0.0f);
+		float hitId = 0.0f;
+		bool hit = false;
+		if (working && P.ray_mode != RESTIR_RAY_MODE_BVH)
+		{
+			hit = g.traceScreenSpaceRay(rayOrigin, direction, g.kMaxRayDistance(), hitPosition);
+		}
+		bool needBvh = working && !hit && P.ray_mode != RESTIR_RAY_MODE_SCREEN;
+		if (needBvh)
+		{
+			float queueDistance;
+			int queueTriangle = traceBvh(g.bvh, rayOrigin, direction, g.kMaxBvhRayDistance(), false, queueDistance,
+				g.stack, g.stackStride);
+			if (queueTriangle >= 0)
+			{
+				hit = true;
+				hitPosition = rayOrigin + direction * queueDistance;
+				hitId = g.encodeSampleId(queueTriangle, direction);
+			}
+			else if (skyEnabled(P))
+			{
+				hit = true;
+				hitPosition = direction;
+				hitId = kSkySampleId;
+			}
+		}
+		V3 contribution = v3s(0.0f);
+		V3 hitNormal = v3s(0.0f);
+		bool evaluated = false;
+		if (hit)
+		{
+			evaluated = g.evaluateSample(position, normal, albedo, hitPosition, hitId, contribution, hitNormal);
+		}
+		if (evaluated)
+		{
+			float target = luminance(contribution);
+			float sourcePdf = dot(normal, direction) / kPi;
+			if (!isSkySample(hitId))
+			{
+				V3 fromReceiver = hitPosition - position;
+				V3 fromOrigin = hitPosition - rayOrigin;
+				float receiverSquared = fmaxf(dot(fromReceiver, fromReceiver), g.kMinDistanceSquared() * 0.01f);
+				float originSquared = fmaxf(dot(fromOrigin, fromOrigin), g.kMinDistanceSquared() * 0.01f);
+				float hitCosineOrigin = fmaxf(-dot(hitNormal, fromOrigin), 0.0f) * inversesqrt(originSquared);
+				float hitCosineReceiver = -dot(hitNormal, fromReceiver) * inversesqrt(receiverSquared);
+				sourcePdf = hitCosineReceiver > 0.0001f
+					? sourcePdf * (hitCosineOrigin / originSquared) * (receiverSquared / hitCosineReceiver)
+					: 0.0f;
+			}
+			if (target > 0.0f && sourcePdf > 0.0001f)
+			{
+				updateReservoir(canonical, contribution, hitPosition, hitNormal, hitId, target, target / sourcePdf, randomSelect);
+			}
+		}
+	}
+
+	const float canonicalWeight = canonical.target > 0.000001f ? canonical.weightSum / (canonical.count * canonical.target) : 0.0f;
+	const bool historyValid = P.history_valid > 0.5f;
+	V2 previousUv = v2(0.0f, 0.0f);
+	const V4 clipPrevious = mul(P.prev_view_proj, v4(position, 1.0f));
+	if (clipPrevious.w > 0.0001f)
+	{
+		previousUv = clipToUv(P, clipPrevious);
+	}
+	const float radius = g.reuseRadius(position);
+	PairwiseMis mis = g.beginPairwiseMis(position, normal, canonical, canonical.count, P.temporal_taps);
+	float combinedWeight = 0.0f;
+	if (working)
+	{
+		for (int tapIndex = 0; tapIndex < P.temporal_taps; ++tapIndex)
+		{
+			float random0 = nextRandom(rng);
+			float random1 = nextRandom(rng);
+			float random2 = nextRandom(rng);
+			float randomSelect = nextRandom(rng);
+			V2 historyUv = v2(-1.0f, -1.0f);
+			if (historyValid)
+			{
+				if (g.grid.worldSpace)
+				{
+					uint32_t entry = gridPickEntry(g.grid, position, normal, random0, random1, random2);
+					if (entry != kGridInvalid)
+					{
+						historyUv = g.giPixelUv(entry);
+					}
+				}
+				else if (tapIndex == 0 && clipPrevious.w > 0.0001f)
+				{
+					historyUv = previousUv;
+				}
+			}
+			NeighbourReservoir neighbour;
+			bool accepted = false;
+			if (isOnScreen(historyUv))
+			{
+				int i = g.gi(historyUv);
+				accepted = g.acceptNeighbour(f4(__ldg(b.historySample + i)), f4(__ldg(b.historyReceiver + i)),
+					f4(__ldg(b.historyNormal + i)), position, normal, radius, neighbour);
+			}
+			if (!accepted)
+			{
+				GiPass::skipNeighbour(mis);
+				continue;
+			}
+			g.addNeighbour(mis, position, normal, albedo, neighbour, randomSelect);
+		}
+		combinedWeight = g.finishPairwiseMis(mis, position, normal, canonical, canonicalWeight, nextRandom(rng));
+	}
+
+	// Boiling filter: the group's mean estimate, summed as compute.sh's tree.
+	const float estimate = working ? mis.combined.target * combinedWeight : 0.0f;
+	float sumEstimate = estimate;
+	float sumWorking = working ? 1.0f : 0.0f;
+	for (int stride = 16; stride > 0; stride >>= 1)
+	{
+		float e = __shfl_down_sync(0xffffffffu, sumEstimate, stride);
+		float c = __shfl_down_sync(0xffffffffu, sumWorking, stride);
+		if (lane < stride)
+		{
+			sumEstimate += e;
+			sumWorking += c;
+		}
+	}
+	sumEstimate = __shfl_sync(0xffffffffu, sumEstimate, 0);
+	sumWorking = __shfl_sync(0xffffffffu, sumWorking, 0);
+	const float tileMean = sumEstimate / fmaxf(sumWorking, 1.0f);
+	if (working && P.boiling_filter > 0.0f && combinedWeight > 0.0f)
+	{
+		float reference = canonical.target * canonicalWeight;
+		V3 historyColor;
+		if (historyValid && g.historyIrradiance(previousUv, position, normal, historyColor))
+		{
+			reference = fmaxf(reference, luminance(historyColor * albedo));
+		}
+		else
+		{
+			reference = fmaxf(reference, tileMean);
+		}
+		float limit = P.boiling_filter * reference;
+		if (estimate > limit)
+		{
+			combinedWeight *= limit / estimate;
+		}
+	}
+	if (inside)
+	{
+		const int i = py * g.w + px;
+		b.outSample[i] = working ? make_float4(mis.combined.position.x, mis.combined.position.y, mis.combined.position.z,
+			mis.totalCount) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+		b.outReceiver[i] = working ? make_float4(position.x, position.y, position.z, combinedWeight)
+			: make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+		b.outNormal[i] = working ? make_float4(normal.x, normal.y, normal.z, mis.combined.id) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+	}
+}
+
+__global__ void __launch_bounds__(128) giSpatialKernel(const RestirParams P, BvhView bvh, GiBindings b)
+{
+	const int px = int(blockIdx.x * 16 + threadIdx.x % 16);
+	const int py = int(blockIdx.y * 8 + threadIdx.x / 16);
+	GiPass g = makePass(P, bvh, b, P.camera_position, nullptr, 0);
+	if (px >= g.w || py >= g.h)
+	{
+		return;
+	}
+	const int outIndex = py * g.w + px;
+	const V2 uv = pixelUv(px, py, g.giTexel);
+	const float depth = g.depthAt(uv);
+	if (depth >= kSkyDepth)
+	{
+		storeH4(b.outColor, outIndex, v4(0.0f, 0.0f, 0.0f, 0.0f));
+		storeH4(b.outMoments, outIndex, v4(0.0f, 0.0f, 0.0f, 0.0f));
+		return;
+	}
+	const V3 position = reconstructWorldPosition(P, uv, depth);
+	const V3 normal = g.decode(uv);
+	const V3 albedo = g.diffuseAlbedo(uv);
+	const V2 pixel = v2(floorf(uv.x * g.giSize.x), floorf(uv.y * g.giSize.y));
+	const uint32_t pixelIndex = uint32_t(pixel.y) * uint32_t(g.giSize.x) + uint32_t(pixel.x);
+	uint32_t rng = pcg(uint32_t(pixel.x) + pcg(uint32_t(pixel.y) + pcg(uint32_t(P.frame_index) ^ 0x68e31da4u)));
+
+	const int own = g.gi(uv);
+	const V4 ownSample = f4(b.reservoirSample[own]);
+	const float canonicalWeight = b.reservoirReceiver[own].w;
+	const float ownId = b.reservoirNormal[own].w;
+	const float canonicalCount = fmaxf(fminf(ownSample.w, 20.0f), 1.0f);
+	GiReservoir canonical = emptyReservoir();
+	V3 canonicalContribution = v3s(0.0f);
+	V3 canonicalNormal = v3(0.0f, 0.0f, 1.0f);
+	bool canonicalValid = false;
+	if (canonicalWeight > 0.0f)
+	{
+		canonicalValid = g.evaluateSample(position, normal, albedo, ownSample.xyz(), ownId, canonicalContribution, canonicalNormal);
+	}
+	if (canonicalValid)
+	{
+		canonical.contribution = canonicalContribution;
+		canonical.position = ownSample.xyz();
+		canonical.normal = canonicalNormal;
+		canonical.id = ownId;
+		canonical.target = luminance(canonicalContribution);
+	}
+
+	const float radius = g.reuseRadius(position);
+	PairwiseMis mis = g.beginPairwiseMis(position, normal, canonical, canonicalCount, P.spatial_taps);
+	for (int tapIndex = 0; tapIndex < P.spatial_taps; ++tapIndex)
+	{
+		float random0 = nextRandom(rng);
+		float random1 = nextRandom(rng);
+		float random2 = nextRandom(rng);
+		float randomSelect = nextRandom(rng);
+		V2 neighbourUv = v2(-1.0f, -1.0f);
+		if (g.grid.worldSpace)
+		{
+			uint32_t entry = gridPickEntry(g.grid, position, normal, random0, random1, random2);
+			if (entry != kGridInvalid && entry != pixelIndex)
+			{
+				neighbourUv = g.giPixelUv(entry);
+			}
+		}
+		else
+		{
+			float diskRadius = 12.0f * sqrtf(random0);
+			float angle = 2.0f * kPi * random1;
+			float sn, cs;
+			rn_sincos(angle, &sn, &cs);
+			V2 neighbourPixel = v2(floorf(pixel.x + cs * diskRadius), floorf(pixel.y + sn * diskRadius));
+			if (neighbourPixel.x != pixel.x || neighbourPixel.y != pixel.y)
+			{
+				neighbourUv = v2((neighbourPixel.x + 0.5f) * g.giTexel.x, (neighbourPixel.y + 0.5f) * g.giTexel.y);
+			}
+		}
+		NeighbourReservoir neighbour;
+		bool accepted = false;
+		if (isOnScreen(neighbourUv))
+		{
+			int i = g.gi(neighbourUv);
+			accepted = g.acceptNeighbour(f4(b.reservoirSample[i]), f4(b.reservoirReceiver[i]), f4(b.reservoirNormal[i]),
+				position, normal, radius, neighbour);
+		}
+		if (!accepted)
+		{
+			GiPass::skipNeighbour(mis);
+			continue;
+		}
+		g.addNeighbour(mis, position, normal, albedo, neighbour, randomSelect);
+	}
+
+	const float combinedWeight = g.finishPairwiseMis(mis, position, normal, canonical, canonicalWeight, nextRandom(rng));
+	V3 estimate = mis.combined.contribution * combinedWeight;
+	if (P.outlier_clamp > 0.0f)
+	{
+		estimate = vmin(estimate, v3s(P.outlier_clamp));
+	}
+	const V3 irradiance = estimate / vmax(albedo, v3s(0.001f));
+	const float irradianceLuminance = luminance(irradiance);
+
+	V3 previousColor = v3s(0.0f);
+	V3 previousMoments = v3s(0.0f);
+	const V4 clipPrevious = mul(P.prev_view_proj, v4(position, 1.0f));
+	if (P.history_valid > 0.5f && clipPrevious.w > 0.0001f)
+	{
+		// reprojectHistory (cs_restir_spatial.sc:49-93)
+		const V2 previousUv = clipToUv(P, clipPrevious);
+		V3 c = v3s(0.0f);
+		V3 m = v3s(0.0f);
+		const V2 texelCoord = v2(previousUv.x * g.giSize.x - 0.5f, previousUv.y * g.giSize.y - 0.5f);
+		const V2 baseCoord = v2(floorf(texelCoord.x), floorf(texelCoord.y));
+		const V2 blend = texelCoord - baseCoord;
+		float weightSum = 0.0f;
+		for (int tapIndex = 0; tapIndex < 4; ++tapIndex)
+		{
+			const V2 offset = v2(float(tapIndex & 1), float(tapIndex >> 1));
+			const V2 tapUv = v2((baseCoord.x + offset.x + 0.5f) * g.giTexel.x, (baseCoord.y + offset.y + 0.5f) * g.giTexel.y);
+			if (!isOnScreen(tapUv))
+			{
+				continue;
+			}
+			const int i = g.gi(tapUv);
+			if (!g.sameHistorySurface(i, position, normal))
+			{
+				continue;
+			}
+			const V2 bilinear = v2(mixf(1.0f - blend.x, blend.x, offset.x), mixf(1.0f - blend.y, blend.y, offset.y));
+			const float weight = bilinear.x * bilinear.y;
+			c = c + loadH4(b.historyColor, i).xyz() * weight;
+			m = m + loadH4(b.historyMoments, i).xyz() * weight;
+			weightSum += weight;
+		}
+		if (weightSum < 0.01f)
+		{
+			c = v3s(0.0f);
+			m = v3s(0.0f);
+		}
+		else
+		{
+			c = c / weightSum;
+			m = m / weightSum;
+		}
+		previousColor = c;
+		previousMoments = m;
+	}
+	const float historyLength = fminf(previousMoments.z + 1.0f, 16.0f);
+	const float blendWeight = 1.0f / historyLength;
+	const V3 color = mix(previousColor, irradiance, blendWeight);
+	const float m0 = mixf(previousMoments.x, irradianceLuminance, blendWeight);
+	const float m1 = mixf(previousMoments.y, irradianceLuminance * irradianceLuminance, blendWeight);
+	storeH4(b.outColor, outIndex, v4(color, historyLength));
+	storeH4(b.outMoments, outIndex, v4(m0, m1, historyLength, 0.0f));
+}
+
+GiBindings bindings(const RestirGBuffer* gb, const RestirGiHistory* history, const uint32_t* grid, const float* shadowAtlas,
+	const uint16_t* surfaceLight)
+{
+	GiBindings b = {};
+	b.albedo = gb->albedo;
+	b.normal = gb->normal;
+	b.depth = gb->depth;
+	b.historySample = reinterpret_cast<const float4*>(history->sample);
+	b.historyReceiver = reinterpret_cast<const float4*>(history->receiver);
+	b.historyNormal = reinterpret_cast<const float4*>(history->normal);
+	b.historyColor = history->color;
+	b.historyMoments = history->moments;
+	b.surfaceLight = surfaceLight;
+	b.shadowAtlas = shadowAtlas;
+	b.grid = grid;
+	return b;
+}
+
+bool validCommon(const RestirParams* p, const RestirScene* s, const RestirGBuffer* gb, const RestirGiHistory* h,
+	const uint32_t* grid, const float* atlas)
+{
+	return p != nullptr && s != nullptr && gb != nullptr && h != nullptr && grid != nullptr && atlas != nullptr
+		&& gb->albedo != nullptr && gb->normal != nullptr && gb->depth != nullptr && h->receiver != nullptr
+		&& h->normal != nullptr && h->color != nullptr && p->gi_width > 0 && p->gi_height > 0 && p->trace_steps > 0
+		&& p->grid_table_size >= 4u && (p->grid_table_size & (p->grid_table_size - 1u)) == 0u;
+}
+
+} // namespace
+} // namespace restir
+
+using namespace restir;
+
+extern "C" int restir_gi_temporal(const RestirParams* params, const RestirScene* scene, const RestirGBuffer* gbuffer,
+	const RestirGiHistory* history, const uint32_t* previous_grid, const float* shadow_atlas, const uint16_t* surface_light,
+	const RestirGiReservoirs* output, void* stream)
+{
+	if (!validCommon(params, scene, gbuffer, history, previous_grid, shadow_atlas) || history->sample == nullptr
+		|| output == nullptr || output->sample == nullptr || output->receiver == nullptr || output->normal == nullptr)
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	GiBindings b = bindings(gbuffer, history, previous_grid, shadow_atlas, surface_light);
+	b.outSample = reinterpret_cast<float4*>(output->sample);
+	b.outReceiver = reinterpret_cast<float4*>(output->receiver);
+	b.outNormal = reinterpret_cast<float4*>(output->normal);
+	const int groups = int((params->gi_width + 3) / 4 * ((params->gi_height + 7) / 8));
+	giTemporalKernel<<<(groups + kGiWarps - 1) / kGiWarps, kGiThreads, 0, asStream(stream)>>>(*params, makeBvhView(scene), b);
+	return launchStatus();
+}
+
+extern "C" int restir_gi_spatial(const RestirParams* params, const RestirScene* scene, const RestirGBuffer* gbuffer,
+	const RestirGiReservoirs* current, const uint32_t* current_grid, const RestirGiHistory* history, const float* shadow_atlas,
+	const uint16_t* surface_light, uint16_t* color, uint16_t* moments, void* stream)
+{
+	if (!validCommon(params, scene, gbuffer, history, current_grid, shadow_atlas) || current == nullptr
+		|| current->sample == nullptr || current->receiver == nullptr || current->normal == nullptr || color == nullptr
+		|| moments == nullptr || history->moments == nullptr)
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	GiBindings b = bindings(gbuffer, history, current_grid, shadow_atlas, surface_light);
+	b.reservoirSample = reinterpret_cast<const float4*>(current->sample);
+	b.reservoirReceiver = reinterpret_cast<const float4*>(current->receiver);
+	b.reservoirNormal = reinterpret_cast<const float4*>(current->normal);
+	b.outColor = color;
+	b.outMoments = moments;
+	dim3 grid((params->gi_width + 15) / 16, (params->gi_height + 7) / 8);
+	giSpatialKernel<<<grid, 128, 0, asStream(stream)>>>(*params, makeBvhView(scene), b);
+	return launchStatus();
+}

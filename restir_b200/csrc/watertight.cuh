@@ -90,83 +90,14 @@ __device__ __forceinline__ float intersectWatertight(const WatertightRay& r, V3 
 	return t / det;
 }
 
-// Nearest watertight hit in (0, distance], ties to the lower triangle index;
-// full stack, nearest child first.
+// Nearest watertight hit in (0, distance], ties to the lower triangle index,
+// with conservative box tests.
 __device__ inline int traceWatertight(const BvhView& b, V3 o, V3 d, float& distance)
 {
-	WatertightRay ray = makeWatertightRay(o, d);
-	V3 inv = bvhInverseDirection(d);
-	if (!b.available() || intersectBox(o, inv, b.row(0).xyz(), b.row(1).xyz(), distance) < 0.0f)
-	{
-		return -1;
-	}
-	int stack[64];
-	int top = 0;
-	int hit = -1;
-	int node = 0;
-	for (int step = 0; step < (1 << 24); ++step)
-	{
-		V4 node0 = b.row(node * 2);
-		V4 node1 = b.row(node * 2 + 1);
-		if (node1.w >= 0.0f)
-		{
-			int first = int(node0.w);
-			int count = int(node1.w);
-			for (int t = first; t < first + count; ++t)
-			{
-				float h = intersectWatertight(ray, b.vertex(t, 0), b.vertex(t, 1), b.vertex(t, 2), distance);
-				if (h > 0.0f && (h < distance || (h == distance && (hit < 0 || t < hit))))
-				{
-					distance = h;
-					hit = t;
-				}
-			}
-		}
-		else
-		{
-			int left = node + 1;
-			int right = int(node0.w);
-			float leftDistance = intersectBox(o, inv, b.row(left * 2).xyz(), b.row(left * 2 + 1).xyz(), distance);
-			float rightDistance = intersectBox(o, inv, b.row(right * 2).xyz(), b.row(right * 2 + 1).xyz(), distance);
-			bool visitLeft = leftDistance >= 0.0f;
-			bool visitRight = rightDistance >= 0.0f;
-			if (visitLeft && visitRight)
-			{
-				bool leftFirst = leftDistance <= rightDistance;
-				if (top < 64)
-				{
-					stack[top++] = leftFirst ? right : left;
-				}
-				else
-				{
-					raiseStatus(1u);
-				}
-				node = leftFirst ? left : right;
-				continue;
-			}
-			if (visitLeft || visitRight)
-			{
-				node = visitLeft ? left : right;
-				continue;
-			}
-		}
-		bool found = false;
-		while (top > 0)
-		{
-			int candidate = stack[--top];
-			if (intersectBox(o, inv, b.row(candidate * 2).xyz(), b.row(candidate * 2 + 1).xyz(), distance) >= 0.0f)
-			{
-				node = candidate;
-				found = true;
-				break;
-			}
-		}
-		if (!found)
-		{
-			break;
-		}
-	}
-	return hit;
+	const WatertightRay ray = makeWatertightRay(o, d);
+	return traceNearestFirst(b, o, d, distance, true,
+		[&](int t, float tmax) { return intersectWatertight(ray, b.vertex(t, 0), b.vertex(t, 1), b.vertex(t, 2), tmax); },
+		[](int) { return true; });
 }
 
 } // namespace restir

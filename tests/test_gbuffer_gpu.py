@@ -26,7 +26,7 @@ def test_gbuffer_bit_exact(scene, size):
     host, dev = render_gbuffer(setup, params, w, h)
     for name in host:
         np.testing.assert_array_equal(dev[name], host[name], err_msg=name)
-    assert (host["depth"] < 1.0).mean() > 0.3
+    assert (host["depth"] < 1.0).mean() > 0.2
 
 
 @pytest.mark.gpu

@@ -69,8 +69,11 @@ def test_watertight_agrees_with_moeller_trumbore_off_edges():
     ids_mt, t_mt, _, _ = trace_both(setup, rays, rb.TRACE_CLOSEST)
     ids_wt, t_wt, _, _ = trace_both(setup, rays, rb.TRACE_CLOSEST_WATERTIGHT)
     both = (ids_mt >= 0) & (ids_wt >= 0)
-    assert (ids_mt == ids_wt).mean() > 0.999
-    np.testing.assert_allclose(t_wt[both & (ids_mt == ids_wt)], t_mt[both & (ids_mt == ids_wt)], rtol=1e-5)
+    # Where the two tests pick different triangles, the scene has coplanar
+    # faces (box bottoms on the ground): the distances still agree.
+    assert (ids_mt == ids_wt).mean() > 0.98
+    assert ((ids_mt >= 0) == (ids_wt >= 0)).mean() > 0.9999
+    np.testing.assert_allclose(t_wt[both], t_mt[both], rtol=1e-5)
 
 
 @pytest.mark.gpu
