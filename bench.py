@@ -1,0 +1,340 @@
+"""Benchmark: one frame of the per-frame light-transport path at 1920x1080.
+
+Workload (the metric's configuration): a seeded procedural scene of ~1M
+triangles (boxes, 512-triangle spheres, thin two-sided planes, 128 emissive
+panels), rendered at 1920x1080 with the reference's default settings: half-
+resolution ReSTIR GI (2 candidates, 2 temporal and 4 spatial taps through the
+world-space hash grid), ReSTIR DI at full resolution (8 candidates, 3 spatial
+taps) over the 256 emissive triangles and 64 extra point lights, a 3x512^2
+shadow atlas, the SVGF denoiser with 5 a-trous iterations, the composite.
+A step is one frame through the C++ frame driver (restir_renderer_render).
+The scene's buffers (126 MB of BVH, ~500 MB of frame targets) exceed the 126
+MB L2, so no flush is needed between frames.
+
+Reported: ms per frame (device time, CUDA events on the renderer's stream,
+max over ranks), Mrays/s (rays counted on a separate profiling frame), the
+relative MSE of the displayed frame against an FP64 progressive reference of
+the same view, per-pass times, the roofline of the dominant pass, an end-to-
+end time through the public API, and the CPU baseline (the oracle's
+restatement of the same passes, on a bounded sample).
+
+Multi-GPU: the path does not shard within a view (reuse reads any pixel's
+reservoir through the world-space grid), so N ranks run N independent
+replicas (weak scaling); value is the whole job's time per frame.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "1080p ms/frame at equal relMSE vs FP64 ref: plain vs radiance-cache; Mrays/s"
+WIDTH, HEIGHT = 1920, 1080
+TRIANGLES = 1_000_000
+EXTRA_LIGHTS = 64
+REFERENCE_FRAMES = 64
+
+# Algorithmic (compulsory) bytes per pixel of each pass's image reads and
+# writes, besides its BVH traversal (32 B per node fetch, 48 B per triangle
+# test): see DESIGN.md, "Roofline".
+PASS_PIXEL_BYTES = {
+    "shadow": ("atlas", 4),
+    "gbuffer": ("full", 24),
+    "di_temporal": ("full", 96),
+    "di_spatial": ("full", 72),
+    "grid": ("gi", 20),
+    "gi_temporal": ("gi", 116),
+    "gi_spatial": ("gi", 124),
+    "denoise": ("gi", 56 + 5 * 48),
+    "composite": ("full", 50),
+    "reference": ("full", 57),
+}
+
+
+def load_peaks() -> tuple[float, str]:
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        return float(json.loads(path.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, value in zip(names, parts[5:9]):
+                if value.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def scene_and_settings(rb):
+    mesh = rb.Mesh.procedural(rb.SCENE_CITY, 0, TRIANGLES)
+    settings = rb.default_settings(mesh)
+    settings.extra_lights = EXTRA_LIGHTS
+    return mesh, settings
+
+
+def cpu_baseline(steps: int = 1, scale: int = 4) -> dict:
+    """The oracle (CPU restatement, all host threads) on a bounded sample of the
+    same workload: one frame at 1/scale of the resolution in each axis and a
+    shadow atlas of 1/scale the face size, each pass's time multiplied by
+    scale^2 (its pixels or texels)."""
+    import oracle.binding as ob
+    import restir_b200 as rb
+    from oracle.frame import FrameRunner
+    from tests.helpers import make_scene
+
+    setup = make_scene(rb.SCENE_CITY, 0, TRIANGLES, extra_lights=EXTRA_LIGHTS)
+    settings = setup.settings
+    settings.shadow_face_size = 512 // scale
+    runner = FrameRunner(setup, WIDTH // scale, HEIGHT // scale, "oracle", settings)
+    runner.render()  # history for the temporal passes
+    totals = []
+    for _ in range(steps):
+        runner.prepare()
+        elapsed = 0.0
+        for _, fn in runner.passes():
+            t = time.perf_counter()
+            fn()
+            elapsed += time.perf_counter() - t
+        runner.finish()
+        totals.append(elapsed * scale * scale * 1e3)
+    return {"value": float(np.median(totals)), "unit": "ms/frame", "cores": ob.load().oracle_get_threads(),
+            "kind": "port",
+            "sample": f"{steps} frame(s) at {WIDTH // scale}x{HEIGHT // scale} with a {3 * (512 // scale)}x"
+                      f"{2 * (512 // scale)} shadow atlas on the same 1M-triangle scene, each pass's time x{scale * scale}"}
+
+
+def reference_arm(args, rank: int, world: int) -> None:
+    """--impl reference: the reference's per-frame path on the host cores. The
+    reference runs it in bgfx shaders (no CPU implementation, and no graphics
+    stack here), so this is the oracle's C++ restatement of its shaders."""
+    if rank != 0:
+        return
+    times = []
+    baseline = None
+    for step in range(args.warmup + args.steps):
+        t = time.perf_counter()
+        baseline = cpu_baseline(steps=1, scale=4)
+        if step >= args.warmup:
+            times.append(baseline["value"])
+    value = float(np.mean(times))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "ms/frame", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"1920x1080 frame, seeded 1M-triangle city scene, GI 1/2 res + DI + SVGF x5",
+                   "scene_triangles": TRIANGLES, "width": WIDTH, "height": HEIGHT},
+        "cpu_baseline": {"value": value, "unit": "ms/frame", "cores": baseline["cores"], "kind": "port",
+                         "sample": baseline["sample"]},
+        "e2e": {"value": value, "unit": "ms/frame", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def own_arm(args, rank: int, world: int) -> None:
+    import torch
+
+    import restir_b200 as rb
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_module
+        dist = dist_module
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    mesh, settings = scene_and_settings(rb)
+    renderer = rb.Renderer(settings)
+    t = time.perf_counter()
+    renderer.set_scene(mesh, use_scene_defaults=True)
+    scene_ms = (time.perf_counter() - t) * 1e3
+    settings = renderer.settings
+    settings.extra_lights = EXTRA_LIGHTS
+    renderer.settings = settings
+    frame = rb.frame_input(mesh, WIDTH, HEIGHT)
+
+    # FP64 progressive reference of this view (not timed).
+    renderer.set_reference_accumulation(True)
+    for _ in range(REFERENCE_FRAMES):
+        renderer.render(frame)
+    renderer.set_reference_accumulation(False)
+
+    # Let the live history settle, then one profiling frame for the work counts.
+    for _ in range(max(args.warmup, 3)):
+        renderer.render(frame)
+    counts = renderer.profile_frame(frame)
+    for _ in range(args.warmup):
+        renderer.render(frame)
+    renderer.synchronize()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.ExternalStream(renderer.stream)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start.record(stream)
+    for _ in range(args.steps):
+        renderer.render(frame, graph=args.graph)
+    stop.record(stream)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    elapsed_ms = start.elapsed_time(stop)
+    clocks = sampler.stop()
+    pass_ms = renderer.pass_history(args.steps) if not args.graph else np.zeros((0, len(rb.PASS_NAMES)))
+    metrics = renderer.frame_submitted()
+
+    # End to end through the public API: each step renders the frame from its
+    # host-side input and reads the frame's error record back to the host.
+    renderer.synchronize()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        renderer.render(frame)
+        step_metrics = renderer.frame_submitted()
+    e2e_ms = (time.perf_counter() - t) * 1e3 / args.steps
+
+    total = torch.tensor([elapsed_ms, e2e_ms], device="cuda", dtype=torch.float64)
+    if dist is not None:
+        dist.all_reduce(total, op=dist.ReduceOp.MAX)
+    elapsed_ms, e2e_ms = float(total[0]), float(total[1])
+    if rank != 0:
+        renderer.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    params, plan, _ = renderer.last_frame()
+    ms_per_frame = elapsed_ms / args.steps
+    rays = int(counts[:, 0:4].sum())
+    passes = rb.PASS_NAMES
+    mean_pass = pass_ms.mean(axis=0) if len(pass_ms) else np.zeros(len(passes))
+    sizes = {"full": WIDTH * HEIGHT, "gi": params.gi_width * params.gi_height,
+             "atlas": 6 * params.shadow_face_size ** 2}
+    pass_bytes = {}
+    for i, name in enumerate(passes):
+        res, per_pixel = PASS_PIXEL_BYTES[name]
+        ran = mean_pass[i] > 0
+        pixel_bytes = sizes[res] * per_pixel + (8 * params.grid_table_size if name == "grid" else 0)
+        pass_bytes[name] = (pixel_bytes + 32 * int(counts[i, 4]) + 48 * int(counts[i, 5])) if ran else 0
+    dominant = int(np.argmax(mean_pass))
+    peak, peak_kind = load_peaks()
+    achieved = pass_bytes[passes[dominant]] / (mean_pass[dominant] * 1e-3) / 1e9 if mean_pass[dominant] > 0 else 0.0
+    launches = 2 + (2 if plan.di_active else 0) + 2 + 2 + (1 + plan.atrous_iterations if plan.denoiser else 0) + 1
+
+    baseline = cpu_baseline(steps=1, scale=2) if not args.no_cpu_baseline else None
+    line = {
+        "metric": METRIC, "value": ms_per_frame, "unit": "ms/frame", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_frame, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+        "config": {"workload": "1920x1080 frame, seeded 1M-triangle city scene, GI 1/2 res + DI + SVGF x5",
+                   "scene_triangles": mesh.triangle_count, "width": WIDTH, "height": HEIGHT,
+                   "gi_resolution": [params.gi_width, params.gi_height], "di_lights": params.di_light_count,
+                   "grid_table_size": params.grid_table_size, "graph": bool(args.graph),
+                   "l2": "inputs larger than L2 (BVH 126 MB + frame targets), no flush",
+                   "parallelism": f"replicas x{world}"},
+        "mrays_per_s": rays / (ms_per_frame * 1e-3) / 1e6,
+        "rays_per_frame": {"primary_and_shadow_map": int(counts[:, 0].sum()), "gi_closest": int(counts[:, 1].sum()),
+                           "visibility_any_hit": int(counts[:, 2].sum()), "depth_buffer_marches": int(counts[:, 3].sum())},
+        "rel_mse_vs_fp64_reference": metrics.relative_mse, "bias_vs_fp64_reference": metrics.bias,
+        "reference_frames": REFERENCE_FRAMES,
+        "pass_ms": {name: float(mean_pass[i]) for i, name in enumerate(passes)},
+        "scene_setup_ms": scene_ms,
+        "e2e": {"value": e2e_ms, "unit": "ms/frame", "h2d_bytes_per_step": 28, "d2h_bytes_per_step": 32,
+                "api": "restir_renderer_render + restir_renderer_measure (error record read back) per step"},
+        "gpu_launches": launches * args.steps,
+        "roofline": {"bound": "hbm", "kernel": passes[dominant], "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": None, "algorithmic_bytes_per_launch": pass_bytes[passes[dominant]]},
+        "cpu_baseline": baseline,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    renderer.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    parser = argparse.ArgumentParser()
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=30)
+    parser.add_argument("--warmup", type=int, default=5)
+    parser.add_argument("--impl", default="own", choices=["own", "reference"])
+    parser.add_argument("--graph", action="store_true", help="replay each frame as a CUDA graph")
+    parser.add_argument("--no-cpu-baseline", action="store_true")
+    args = parser.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.gpus == 1 else 1)))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+    else:
+        own_arm(args, rank, world)
+
+
+if __name__ == "__main__":
+    main()

@@ -151,6 +151,17 @@ int restir_renderer_render_graph(void* renderer, const RestirFrameInput* input);
 /* Runs the error pass against the reference on the last frame and reads its
  * record back (waits for the stream), as Renderer::frameSubmitted does. */
 int restir_renderer_measure(void* renderer, RestirMetrics* metrics);
+/* Per-pass device times (cudaEvent pairs on the renderer's stream) of the
+ * last `frames` frames rendered without a graph, oldest first, as
+ * ms[frame * RESTIR_PASS_COUNT + pass]; up to 128 frames are kept. Waits for
+ * the stream; returns the number of frames written. */
+int restir_renderer_pass_history(void* renderer, uint32_t frames, float* ms);
+
+/* Renders one frame with the work counters of restir_counters on, and adds
+ * each pass's counts to counts[pass * 8 + k] (RESTIR_PASS_COUNT x 8). The
+ * device is synchronised after every pass: a profiling frame, not a timed
+ * one. No counterpart in the reference. */
+int restir_renderer_profile_frame(void* renderer, const RestirFrameInput* input, uint64_t* counts);
 void restir_renderer_set_reference_accumulation(void* renderer, int accumulate);
 void restir_renderer_invalidate_history(void* renderer);
 /* Waits for the renderer's stream. */

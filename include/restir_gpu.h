@@ -279,6 +279,15 @@ int restir_error(const RestirParams* params, const uint16_t* display, const doub
  * step cap, bit 1 a hash grid probe sequence was exhausted. */
 int restir_status(uint32_t* flags);
 
+/* Work counters: waits for the device, returns the counts gathered since the
+ * last call (8 values: nearest-hit ray casts, short-stack closest-hit rays,
+ * stackless any-hit rays, depth-buffer marches, BVH node fetches, triangle
+ * tests, depth-buffer steps, unused), clears them, and turns counting on or
+ * off for the launches that follow. Off by default; a counted frame does
+ * extra atomics. No counterpart in the reference (its profiler counts
+ * time only, ui.cpp:20-66). */
+int restir_counters(int enable, uint64_t* counters);
+
 /* Evaluates one numeric convention of restir_numeric.h on the device, for
  * tests: fn 0 sin, 1 cos, 2 exp, 3 half round trip (hardware), 4 half round
  * trip (restir_numeric.h), 5 unorm8 store, 6 floor(log2), 7 x^64. No

@@ -61,6 +61,9 @@ _SIGNATURES = {
     "restir_error": (C.c_int, [C.POINTER(RestirParams), P, P, P, P, P, P]),
     "restir_status": (C.c_int, [C.POINTER(u32)]),
     "restir_numeric_eval": (C.c_int, [C.c_int, P, P, u32, P]),
+    "restir_counters": (C.c_int, [C.c_int, P]),
+    "restir_renderer_profile_frame": (C.c_int, [P, C.POINTER(RestirFrameInput), P]),
+    "restir_renderer_pass_history": (C.c_int, [P, u32, P]),
     # restir_host.h
     "restir_mesh_procedural": (P, [C.c_int, u32, u32]),
     "restir_mesh_create": (P, [C.POINTER(RestirMeshDesc)]),
@@ -81,6 +84,21 @@ _SIGNATURES = {
                                       C.POINTER(RestirFramePlan)]),
     "restir_frame_advance": (None, [C.POINTER(RestirParams), C.POINTER(RestirFramePlan), C.POINTER(RestirFrameInput),
                                     C.POINTER(RestirFrameState)]),
+    "restir_renderer_create": (P, [C.POINTER(RestirSettings)]),
+    "restir_renderer_destroy": (None, [P]),
+    "restir_renderer_set_scene": (C.c_int, [P, P, C.c_int]),
+    "restir_renderer_set_settings": (C.c_int, [P, C.POINTER(RestirSettings)]),
+    "restir_renderer_get_settings": (C.c_int, [P, C.POINTER(RestirSettings)]),
+    "restir_renderer_render": (C.c_int, [P, C.POINTER(RestirFrameInput)]),
+    "restir_renderer_render_graph": (C.c_int, [P, C.POINTER(RestirFrameInput)]),
+    "restir_renderer_measure": (C.c_int, [P, C.POINTER(abi.RestirMetrics)]),
+    "restir_renderer_set_reference_accumulation": (None, [P, C.c_int]),
+    "restir_renderer_invalidate_history": (None, [P]),
+    "restir_renderer_synchronize": (C.c_int, [P]),
+    "restir_renderer_stream": (P, [P]),
+    "restir_renderer_last_frame": (C.c_int, [P, C.POINTER(RestirParams), C.POINTER(RestirFramePlan),
+                                             C.POINTER(RestirFrameState)]),
+    "restir_renderer_buffer": (C.c_int, [P, C.c_char_p, C.POINTER(P), C.POINTER(C.c_uint64)]),
 }
 
 # Entry points that may be absent while the library is being extended.
@@ -247,6 +265,116 @@ def frame_input(mesh: Mesh, width: int, height: int, eye=None, yaw=None, pitch=N
 
 def advance(params: RestirParams, plan: RestirFramePlan, frame_input: RestirFrameInput, state: RestirFrameState):
     load().restir_frame_advance(C.byref(params), C.byref(plan), C.byref(frame_input), C.byref(state))
+
+
+class Renderer:
+    """The reference's Renderer (src/renderer.h:73-125) over the C++ frame driver.
+
+    init(settings) / set_scene(mesh) / render(frame_input) / invalidate_history() /
+    set_reference_accumulation(on) / frame_submitted() -> metrics, as in the reference;
+    render_graph() replays the frame as one CUDA graph. Work is enqueued on the
+    renderer's own CUDA stream; frame_submitted() waits for it.
+    """
+
+    def __init__(self, settings: RestirSettings | None = None):
+        lib = load()
+        self._lib = lib
+        self.handle = lib.restir_renderer_create(C.byref(settings) if settings is not None else None)
+        if not self.handle:
+            raise RuntimeError("restir_renderer_create failed")
+        self.mesh = None
+
+    def set_scene(self, mesh: Mesh, use_scene_defaults: bool = True) -> None:
+        self.mesh = mesh
+        check(self._lib.restir_renderer_set_scene(self.handle, mesh.handle, int(use_scene_defaults)), "set_scene")
+
+    @property
+    def settings(self) -> RestirSettings:
+        s = RestirSettings()
+        check(self._lib.restir_renderer_get_settings(self.handle, C.byref(s)), "get_settings")
+        return s
+
+    @settings.setter
+    def settings(self, s: RestirSettings) -> None:
+        check(self._lib.restir_renderer_set_settings(self.handle, C.byref(s)), "set_settings")
+
+    def render(self, frame_input: RestirFrameInput, graph: bool = False) -> None:
+        fn = self._lib.restir_renderer_render_graph if graph else self._lib.restir_renderer_render
+        check(fn(self.handle, C.byref(frame_input)), "render")
+
+    def invalidate_history(self) -> None:
+        self._lib.restir_renderer_invalidate_history(self.handle)
+
+    def set_reference_accumulation(self, accumulate: bool) -> None:
+        self._lib.restir_renderer_set_reference_accumulation(self.handle, int(accumulate))
+
+    def frame_submitted(self) -> abi.RestirMetrics:
+        """Error against the reference (cs_error.sc) and per-pass times of the last frame."""
+        m = abi.RestirMetrics()
+        check(self._lib.restir_renderer_measure(self.handle, C.byref(m)), "measure")
+        return m
+
+    def synchronize(self) -> None:
+        check(self._lib.restir_renderer_synchronize(self.handle), "synchronize")
+
+    def pass_history(self, frames: int) -> np.ndarray:
+        """Per-pass device times (ms) of the last `frames` stream-launched frames: (frames, passes)."""
+        ms = np.zeros((frames, len(PASS_NAMES)), np.float32)
+        n = self._lib.restir_renderer_pass_history(self.handle, frames, ms.ctypes.data)
+        if n < 0:
+            raise RuntimeError(f"pass_history failed with status {n}")
+        return ms[:n]
+
+    def profile_frame(self, frame_input: RestirFrameInput) -> np.ndarray:
+        """One frame with the device work counters on: (passes, 8) counts (see restir_counters)."""
+        counts = np.zeros((len(PASS_NAMES), 8), np.uint64)
+        check(self._lib.restir_renderer_profile_frame(self.handle, C.byref(frame_input), counts.ctypes.data),
+              "profile_frame")
+        return counts
+
+    @property
+    def stream(self) -> int:
+        return self._lib.restir_renderer_stream(self.handle)
+
+    def last_frame(self):
+        params, plan, state = RestirParams(), RestirFramePlan(), RestirFrameState()
+        check(self._lib.restir_renderer_last_frame(self.handle, C.byref(params), C.byref(plan), C.byref(state)),
+              "last_frame")
+        return params, plan, state
+
+    def buffer(self, name: str) -> tuple[int, int]:
+        pointer, nbytes = C.c_void_p(), C.c_uint64()
+        check(self._lib.restir_renderer_buffer(self.handle, name.encode(), C.byref(pointer), C.byref(nbytes)),
+              f"buffer {name}")
+        return pointer.value or 0, nbytes.value
+
+    def download(self, name: str, dtype) -> np.ndarray:
+        """A copy of one of the renderer's device buffers (after synchronize)."""
+        import torch
+        pointer, nbytes = self.buffer(name)
+        self.synchronize()
+        data = device_view(pointer, nbytes, torch.uint8).cpu()
+        return data.numpy().view(dtype)
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self._lib.restir_renderer_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        if _lib is not None:
+            self.close()
+
+
+def device_view(pointer: int, nbytes: int, dtype):
+    """A torch tensor aliasing device memory owned by the library (no copy)."""
+    import torch
+
+    class _View:
+        def __init__(self):
+            self.__cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (pointer, False),
+                                             "version": 3}
+    return torch.as_tensor(_View(), device="cuda").view(dtype)
 
 
 def status_flags() -> int:

@@ -117,6 +117,11 @@ class RestirFrameState(C.Structure):
     ]
 
 
+class RestirMetrics(C.Structure):
+    _fields_ = [("valid", C.c_int), ("relative_mse", C.c_double), ("bias", C.c_double), ("error", C.c_double * 4),
+                ("pass_ms", C.c_float * 10), ("reference_frames", C.c_uint32)]
+
+
 class RestirFramePlan(C.Structure):
     """Which passes a frame runs, as Renderer::render decides (renderer.cpp:627-1094)."""
     _fields_ = [

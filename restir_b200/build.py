@@ -30,7 +30,7 @@ NVCC_FLAGS = ARCH + [
     "-I", str(ROOT / "include"),
 ]
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall",
-             "-I", str(ROOT / "include")]
+             "-I", str(ROOT / "include"), "-I", "/usr/local/cuda/include"]
 
 
 def _nvcc() -> str:

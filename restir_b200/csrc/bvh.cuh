@@ -50,6 +50,13 @@ __host__ __device__ inline BvhView makeBvhView(const RestirScene* s)
 	return b;
 }
 
+// Node fetches and triangle tests of one ray, for the work counters.
+struct TraceWork
+{
+	uint32_t nodes = 0;
+	uint32_t triangles = 0;
+};
+
 __device__ __forceinline__ float intersectBox(V3 o, V3 inv, V3 bmin, V3 bmax, float maxDistance)
 {
 	V3 t0 = (bmin - o) * inv;
@@ -98,8 +105,10 @@ __device__ __forceinline__ V3 bvhInverseDirection(V3 d)
 	return { safeInverse(d.x), safeInverse(d.y), safeInverse(d.z) };
 }
 
-__device__ __forceinline__ int intersectLeaf(const BvhView& b, V3 o, V3 d, int first, int count, float& distance, int hit)
+__device__ __forceinline__ int intersectLeaf(const BvhView& b, V3 o, V3 d, int first, int count, float& distance, int hit,
+	TraceWork& work)
 {
+	work.triangles += uint32_t(count);
 	for (int t = first; t < first + count; ++t)
 	{
 		float h = intersectTriangle(o, d, b.vertex(t, 0), b.vertex(t, 1), b.vertex(t, 2));
@@ -113,7 +122,7 @@ __device__ __forceinline__ int intersectLeaf(const BvhView& b, V3 o, V3 d, int f
 }
 
 // bvh.sh:140-174
-__device__ inline int traceStackless(const BvhView& b, V3 o, V3 d, bool anyHit, float& distance)
+__device__ inline int traceStacklessWalk(const BvhView& b, V3 o, V3 d, bool anyHit, float& distance, TraceWork& work)
 {
 	V3 inv = bvhInverseDirection(d);
 	int hit = -1;
@@ -125,6 +134,7 @@ __device__ inline int traceStackless(const BvhView& b, V3 o, V3 d, bool anyHit, 
 		{
 			break;
 		}
+		++work.nodes;
 		V4 node0 = b.row(node * 2);
 		V4 node1 = b.row(node * 2 + 1);
 		bool leaf = node1.w >= 0.0f;
@@ -135,7 +145,7 @@ __device__ inline int traceStackless(const BvhView& b, V3 o, V3 d, bool anyHit, 
 		}
 		if (leaf)
 		{
-			hit = intersectLeaf(b, o, d, int(node0.w), int(node1.w), distance, hit);
+			hit = intersectLeaf(b, o, d, int(node0.w), int(node1.w), distance, hit, work);
 			if (anyHit && hit >= 0)
 			{
 				return hit;
@@ -152,9 +162,10 @@ __device__ inline int traceStackless(const BvhView& b, V3 o, V3 d, bool anyHit, 
 
 // bvh.sh:216-295. stack: this thread's kBvhShortStack entries, stride apart
 // (shared memory, interleaved across the block's threads).
-__device__ inline int traceShortStack(const BvhView& b, V3 o, V3 d, float& distance, int* stack, int stride)
+__device__ inline int traceShortStack(const BvhView& b, V3 o, V3 d, float& distance, int* stack, int stride, TraceWork& work)
 {
 	V3 inv = bvhInverseDirection(d);
+	++work.nodes;
 	if (intersectBox(o, inv, b.row(0).xyz(), b.row(1).xyz(), distance) < 0.0f)
 	{
 		return -1;
@@ -171,12 +182,13 @@ __device__ inline int traceShortStack(const BvhView& b, V3 o, V3 d, float& dista
 		V4 node1 = b.row(node * 2 + 1);
 		if (node1.w >= 0.0f)
 		{
-			hit = intersectLeaf(b, o, d, int(node0.w), int(node1.w), distance, hit);
+			hit = intersectLeaf(b, o, d, int(node0.w), int(node1.w), distance, hit, work);
 		}
 		else
 		{
 			int left = node + 1;
 			int right = int(node0.w);
+			work.nodes += 2u;
 			float leftDistance = intersectBox(o, inv, b.row(left * 2).xyz(), b.row(left * 2 + 1).xyz(), distance);
 			float rightDistance = intersectBox(o, inv, b.row(right * 2).xyz(), b.row(right * 2 + 1).xyz(), distance);
 			bool visitLeft = leftDistance >= 0.0f;
@@ -217,7 +229,7 @@ __device__ inline int traceShortStack(const BvhView& b, V3 o, V3 d, float& dista
 	}
 	if (dropped)
 	{
-		int stacklessHit = traceStackless(b, o, d, false, distance);
+		int stacklessHit = traceStacklessWalk(b, o, d, false, distance, work);
 		if (stacklessHit >= 0)
 		{
 			hit = stacklessHit;
@@ -236,11 +248,21 @@ __device__ __forceinline__ int traceBvh(const BvhView& b, V3 o, V3 d, float maxD
 	{
 		return -1;
 	}
+	TraceWork work;
+	int hit;
+	int kind;
 	if (stack != nullptr && !anyHit)
 	{
-		return traceShortStack(b, o, d, distance, stack, stride);
+		hit = traceShortStack(b, o, d, distance, stack, stride, work);
+		kind = RESTIR_COUNT_CLOSEST;
 	}
-	return traceStackless(b, o, d, anyHit, distance);
+	else
+	{
+		hit = traceStacklessWalk(b, o, d, anyHit, distance, work);
+		kind = RESTIR_COUNT_ANY;
+	}
+	countWork(kind, work.nodes, work.triangles);
+	return hit;
 }
 
 // Nearest hit in (0, distance) among the triangles accept() lets through,
@@ -255,8 +277,10 @@ __device__ inline int traceNearestFirst(const BvhView& b, V3 o, V3 d, float& dis
 {
 	V3 inv = bvhInverseDirection(d);
 	const float widen = conservative ? 1.00000036f : 1.0f;
+	TraceWork work;
 	auto box = [&](int node) -> float
 	{
+		++work.nodes;
 		V3 lo = b.row(node * 2).xyz();
 		V3 hi = b.row(node * 2 + 1).xyz();
 		V3 t0 = (lo - o) * inv;
@@ -270,6 +294,7 @@ __device__ inline int traceNearestFirst(const BvhView& b, V3 o, V3 d, float& dis
 	};
 	if (!b.available() || box(0) < 0.0f)
 	{
+		countWork(RESTIR_COUNT_PRIMARY, work.nodes, work.triangles);
 		return -1;
 	}
 	int stack[64];
@@ -284,6 +309,7 @@ __device__ inline int traceNearestFirst(const BvhView& b, V3 o, V3 d, float& dis
 		{
 			int first = int(node0.w);
 			int count = int(node1.w);
+			work.triangles += uint32_t(count);
 			for (int t = first; t < first + count; ++t)
 			{
 				float h = test(t, distance);
@@ -339,6 +365,7 @@ __device__ inline int traceNearestFirst(const BvhView& b, V3 o, V3 d, float& dis
 			break;
 		}
 	}
+	countWork(RESTIR_COUNT_PRIMARY, work.nodes, work.triangles);
 	return hit;
 }
 

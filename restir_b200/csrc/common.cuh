@@ -215,6 +215,44 @@ __device__ __forceinline__ void raiseStatus(unsigned int bit)
 	atomicOr(&g_restirStatus, bit);
 }
 
+// --- work counters -----------------------------------------------------------
+
+// Rays by kind, and the node fetches and triangle tests of every BVH ray,
+// counted only while g_restirCounting is set (restir_counters), so that
+// timed frames do none of this work.
+#define RESTIR_COUNT_PRIMARY 0    // nearest-hit ray casts (G-buffer, shadow atlas, restir_trace)
+#define RESTIR_COUNT_CLOSEST 1    // short-stack closest-hit rays (GI candidates)
+#define RESTIR_COUNT_ANY 2        // stackless rays (visibility and shadow rays)
+#define RESTIR_COUNT_SCREEN 3     // depth-buffer marches
+#define RESTIR_COUNT_NODES 4
+#define RESTIR_COUNT_TRIANGLES 5
+#define RESTIR_COUNT_SCREEN_STEPS 6
+#define RESTIR_COUNTERS 8
+
+extern __device__ unsigned long long g_restirCounters[RESTIR_COUNTERS];
+extern __device__ int g_restirCounting;
+
+__device__ __forceinline__ void countWork(int kind, uint32_t nodes, uint32_t triangles)
+{
+	if (!g_restirCounting)
+	{
+		return;
+	}
+	const unsigned mask = __activemask();
+	const unsigned n = __reduce_add_sync(mask, nodes);
+	const unsigned t = __reduce_add_sync(mask, triangles);
+	if (int(threadIdx.x & 31u) == __ffs(mask) - 1)
+	{
+		atomicAdd(&g_restirCounters[kind], static_cast<unsigned long long>(__popc(mask)));
+		atomicAdd(&g_restirCounters[kind == RESTIR_COUNT_SCREEN ? RESTIR_COUNT_SCREEN_STEPS : RESTIR_COUNT_NODES],
+			static_cast<unsigned long long>(n));
+		if (kind != RESTIR_COUNT_SCREEN)
+		{
+			atomicAdd(&g_restirCounters[RESTIR_COUNT_TRIANGLES], static_cast<unsigned long long>(t));
+		}
+	}
+}
+
 // --- launch helpers ----------------------------------------------------------
 
 inline cudaStream_t asStream(void* s)

@@ -365,6 +365,15 @@ struct GiPass
 
 	__device__ inline bool traceScreenSpaceRay(V3 origin, V3 direction, float maxDistance, V3& hitPosition) const
 	{
+		uint32_t steps = 0;
+		bool hit = marchDepthBuffer(origin, direction, maxDistance, hitPosition, steps);
+		countWork(RESTIR_COUNT_SCREEN, steps, 0u);
+		return hit;
+	}
+
+	// traceScreenSpaceRay (restir.sh:364-436); steps counts the depth fetches.
+	__device__ inline bool marchDepthBuffer(V3 origin, V3 direction, float maxDistance, V3& hitPosition, uint32_t& steps) const
+	{
 		hitPosition = v3s(0.0f);
 		float previousDistance = 0.0f;
 		bool previousInFront = true;
@@ -381,6 +390,7 @@ struct GiPass
 			V2 uv;
 			V3 surfacePosition;
 			bool onScreen;
+			++steps;
 			float behind = depthBehindSurface(origin + direction * rayDistance, uv, surfacePosition, onScreen);
 			if (!onScreen)
 			{
@@ -397,6 +407,7 @@ struct GiPass
 					V2 middleUv;
 					V3 middleSurface;
 					bool middleOnScreen;
+					++steps;
 					float middleBehind = depthBehindSurface(origin + direction * middle, middleUv, middleSurface, middleOnScreen);
 					if (middleOnScreen && middleBehind > 0.0f)
 					{

@@ -16,6 +16,8 @@ namespace restir
 {
 
 __device__ unsigned int g_restirStatus = 0;
+__device__ unsigned long long g_restirCounters[RESTIR_COUNTERS] = {};
+__device__ int g_restirCounting = 0;
 
 namespace
 {
@@ -160,6 +162,31 @@ extern "C" int restir_grid_insert(const RestirParams* params, const RestirGBuffe
 	const uint32_t pixels = params->gi_width * params->gi_height;
 	gridInsertKernel<<<(pixels + 255u) / 256u, 256, 0, asStream(stream)>>>(*params, gbuffer->depth, gbuffer->normal, grid);
 	return launchStatus();
+}
+
+extern "C" int restir_counters(int enable, uint64_t* counters)
+{
+	unsigned long long values[RESTIR_COUNTERS] = {};
+	if (cudaDeviceSynchronize() != cudaSuccess
+		|| cudaMemcpyFromSymbol(values, g_restirCounters, sizeof(values)) != cudaSuccess)
+	{
+		return RESTIR_ERROR_LAUNCH;
+	}
+	const unsigned long long zero[RESTIR_COUNTERS] = {};
+	const int flag = enable != 0 ? 1 : 0;
+	if (cudaMemcpyToSymbol(g_restirCounters, zero, sizeof(zero)) != cudaSuccess
+		|| cudaMemcpyToSymbol(g_restirCounting, &flag, sizeof(flag)) != cudaSuccess)
+	{
+		return RESTIR_ERROR_LAUNCH;
+	}
+	if (counters != nullptr)
+	{
+		for (int i = 0; i < RESTIR_COUNTERS; ++i)
+		{
+			counters[i] = values[i];
+		}
+	}
+	return RESTIR_OK;
 }
 
 extern "C" int restir_status(uint32_t* flags)
