@@ -280,9 +280,11 @@ def own_arm(args, rank: int, world: int) -> None:
         ran = mean_pass[i] > 0
         pixel_bytes = sizes[res] * per_pixel + (8 * params.grid_table_size if name == "grid" else 0)
         pass_bytes[name] = (pixel_bytes + 32 * int(counts[i, 4]) + 48 * int(counts[i, 5])) if ran else 0
+    mean_pass = [float(v) for v in mean_pass]
     dominant = int(np.argmax(mean_pass))
     peak, peak_kind = load_peaks()
-    achieved = pass_bytes[passes[dominant]] / (mean_pass[dominant] * 1e-3) / 1e9 if mean_pass[dominant] > 0 else 0.0
+    achieved = float(pass_bytes[passes[dominant]] / (mean_pass[dominant] * 1e-3) / 1e9) if mean_pass[dominant] > 0 else 0.0
+    share = {name: (mean_pass[i] / ms_per_frame if ms_per_frame > 0 else 0.0) for i, name in enumerate(passes)}
     launches = 2 + (2 if plan.di_active else 0) + 2 + 2 + (1 + plan.atrous_iterations if plan.denoiser else 0) + 1
 
     baseline = cpu_baseline(steps=1, scale=2) if not args.no_cpu_baseline else None
@@ -296,12 +298,17 @@ def own_arm(args, rank: int, world: int) -> None:
                    "grid_table_size": params.grid_table_size, "graph": bool(args.graph),
                    "l2": "inputs larger than L2 (BVH 126 MB + frame targets), no flush",
                    "parallelism": f"replicas x{world}"},
-        "mrays_per_s": rays / (ms_per_frame * 1e-3) / 1e6,
+        "mrays_per_s": float(rays / (ms_per_frame * 1e-3) / 1e6),
         "rays_per_frame": {"primary_and_shadow_map": int(counts[:, 0].sum()), "gi_closest": int(counts[:, 1].sum()),
                            "visibility_any_hit": int(counts[:, 2].sum()), "depth_buffer_marches": int(counts[:, 3].sum())},
         "rel_mse_vs_fp64_reference": metrics.relative_mse, "bias_vs_fp64_reference": metrics.bias,
         "reference_frames": REFERENCE_FRAMES,
         "pass_ms": {name: float(mean_pass[i]) for i, name in enumerate(passes)},
+        "pass_share": share,
+        "pass_algorithmic_gbs": {name: (float(pass_bytes[name] / (mean_pass[i] * 1e-3) / 1e9) if mean_pass[i] > 0 else 0.0)
+                                 for i, name in enumerate(passes)},
+        "work_counts": {"node_fetches": int(counts[:, 4].sum()), "triangle_tests": int(counts[:, 5].sum()),
+                        "depth_buffer_steps": int(counts[:, 6].sum())},
         "scene_setup_ms": scene_ms,
         "e2e": {"value": e2e_ms, "unit": "ms/frame", "h2d_bytes_per_step": 28, "d2h_bytes_per_step": 32,
                 "api": "restir_renderer_render + restir_renderer_measure (error record read back) per step"},
@@ -321,7 +328,7 @@ def own_arm(args, rank: int, world: int) -> None:
 def main():
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
-    parser.add_argument("--steps", type=int, default=30)
+    parser.add_argument("--steps", type=int, default=100)
     parser.add_argument("--warmup", type=int, default=5)
     parser.add_argument("--impl", default="own", choices=["own", "reference"])
     parser.add_argument("--graph", action="store_true", help="replay each frame as a CUDA graph")
