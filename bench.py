@@ -214,6 +214,17 @@ def own_arm(args, rank: int, world: int) -> None:
     renderer.settings = settings
     frame = rb.frame_input(mesh, WIDTH, HEIGHT)
 
+    if args.quick:
+        # Profiling runs: W warm-up frames, then K frames, nothing else.
+        for _ in range(args.warmup):
+            renderer.render(frame)
+        for _ in range(args.steps):
+            renderer.render(frame)
+        renderer.synchronize()
+        print(json.dumps({"quick": True, "frames": args.warmup + args.steps}), flush=True)
+        renderer.close()
+        return
+
     # FP64 progressive reference of this view (not timed).
     renderer.set_reference_accumulation(True)
     for _ in range(REFERENCE_FRAMES):
@@ -333,6 +344,8 @@ def main():
     parser.add_argument("--impl", default="own", choices=["own", "reference"])
     parser.add_argument("--graph", action="store_true", help="replay each frame as a CUDA graph")
     parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--quick", action="store_true",
+                        help="profiling runs: W + K frames of the workload, no reference, no report")
     args = parser.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
