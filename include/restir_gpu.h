@@ -43,6 +43,7 @@ extern "C" {
 #define RESTIR_ERROR_UNSUPPORTED (-4)
 #define RESTIR_ERROR_TIMEOUT (-5)
 #define RESTIR_ERROR_OUT_OF_MEMORY (-6)
+#define RESTIR_ERROR_TOO_LARGE (-7)  /* input beyond a fixed-size variant's limit */
 
 /* Ray modes (shaders/bvh.sh:16-19, settings.h:59-65). */
 #define RESTIR_RAY_MODE_SCREEN 0
@@ -274,6 +275,24 @@ uint64_t restir_error_scratch_bytes(uint32_t width, uint32_t height);
  * scratch: restir_error_scratch_bytes bytes of device memory. */
 int restir_error(const RestirParams* params, const uint16_t* display, const double* mean,
 	const uint8_t* alpha, double* out, void* scratch, void* stream);
+
+/* restir_error for callers that cannot allocate device memory: code running
+ * inside a frame that is being recorded into a CUDA graph (cudaMalloc is not
+ * a stream operation and cannot be captured), hosts such as game engines
+ * whose memory manager owns the whole device budget, and real-time loops that
+ * must never enter the driver's allocator (it can synchronise the device).
+ * No counterpart in the reference. The caller passes only inputs and the
+ * 4-double output; the reduction's partial records live in a 64 KB array
+ * inside the library, which every device that loads the library keeps until
+ * the process exits. Limit: width * height <= 8,388,608 pixels (3840x2160
+ * fits); larger images return RESTIR_ERROR_TOO_LARGE. The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current, so make it before any stream capture. All calls share
+ * the one array: calls whose kernels overlap on the GPU (on two streams, say)
+ * race on it and must be ordered by the caller. Nothing in the array needs
+ * to start at zero; each call overwrites the records it reads. */
+int restir_error_noalloc(const RestirParams* params, const uint16_t* display, const double* mean,
+	const uint8_t* alpha, double* out, void* stream);
 
 /* Reads and clears the device status word: bit 0 a traversal reached its
  * step cap, bit 1 a hash grid probe sequence was exhausted. */

@@ -13,6 +13,8 @@
 // in block order, so the result does not depend on scheduling.
 #include "common.cuh"
 
+#include <mutex>
+
 namespace restir
 {
 namespace
@@ -20,6 +22,14 @@ namespace
 
 constexpr int kErrorBlocks = 148 * 4;
 constexpr int kErrorThreads = 256;
+
+// Scratch of restir_error_noalloc: one FP64 partial record (4 doubles) per
+// block, one block per kNoAllocPixelsPerBlock pixels, at most
+// kNoAllocMaxBlocks blocks (64 KB, resident on every device that loads the
+// library until the process exits).
+constexpr uint32_t kNoAllocPixelsPerBlock = 4096;
+constexpr uint32_t kNoAllocMaxBlocks = 2048;
+static __device__ __align__(256) double g_errorNoAllocScratch[kNoAllocMaxBlocks * 4];
 
 __global__ void __launch_bounds__(256) accumulateKernel(const uint16_t* __restrict__ hdr, double* __restrict__ mean,
 	uint8_t* __restrict__ alpha, uint32_t n, double weight)
@@ -127,6 +137,39 @@ uint64_t errorScratchBytes()
 	return uint64_t(kErrorBlocks) * 4u * sizeof(double);
 }
 
+namespace
+{
+
+// Device address of g_errorNoAllocScratch on each device, looked up once per
+// device with that device current (the symbol's name is only a host-side
+// handle, not an address a kernel can use).
+constexpr int kMaxDevices = 64;
+std::mutex g_noAllocMutex;
+double* g_noAllocScratch[kMaxDevices] = {};
+
+int noAllocScratch(double** scratch)
+{
+	int device = 0;
+	if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kMaxDevices)
+	{
+		return RESTIR_ERROR_LAUNCH;
+	}
+	std::lock_guard<std::mutex> lock(g_noAllocMutex);
+	if (g_noAllocScratch[device] == nullptr)
+	{
+		void* address = nullptr;
+		if (cudaGetSymbolAddress(&address, g_errorNoAllocScratch) != cudaSuccess || address == nullptr)
+		{
+			return RESTIR_ERROR_LAUNCH;
+		}
+		g_noAllocScratch[device] = static_cast<double*>(address);
+	}
+	*scratch = g_noAllocScratch[device];
+	return RESTIR_OK;
+}
+
+} // namespace
+
 } // namespace restir
 
 using namespace restir;
@@ -161,4 +204,35 @@ extern "C" int restir_error(const RestirParams* params, const uint16_t* display,
 		return RESTIR_ERROR_INVALID_ARGUMENT;
 	}
 	return launchError(params, display, mean, alpha, out, static_cast<double*>(scratch), asStream(stream));
+}
+
+// The error pass without caller scratch, for callers that cannot allocate
+// device memory (see include/restir_gpu.h). Same two kernels as
+// restir_error, launched with one block per 4096 pixels so that the partial
+// records fit the library's static array; every block writes its record, so
+// the array needs no clearing between calls.
+extern "C" int restir_error_noalloc(const RestirParams* params, const uint16_t* display, const double* mean,
+	const uint8_t* alpha, double* out, void* stream)
+{
+	if (params == nullptr || display == nullptr || mean == nullptr || alpha == nullptr || out == nullptr
+		|| params->width == 0 || params->height == 0)
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	const uint64_t pixels = uint64_t(params->width) * params->height;
+	if (pixels > uint64_t(kNoAllocPixelsPerBlock) * kNoAllocMaxBlocks)
+	{
+		return RESTIR_ERROR_TOO_LARGE;
+	}
+	double* scratch = nullptr;
+	int status = noAllocScratch(&scratch);
+	if (status != RESTIR_OK)
+	{
+		return status;
+	}
+	const int blocks = int((pixels + kNoAllocPixelsPerBlock - 1) / kNoAllocPixelsPerBlock);
+	cudaStream_t s = asStream(stream);
+	errorPartialKernel<<<blocks, kErrorThreads, 0, s>>>(display, mean, alpha, uint32_t(pixels), scratch);
+	errorFinalKernel<<<1, 32, 0, s>>>(scratch, blocks, out);
+	return launchStatus();
 }
