@@ -23,7 +23,8 @@ from .abi import (RestirBvhDesc, RestirDiReservoirs, RestirFrameInput, RestirFra
                   RestirGBuffer, RestirGiHistory, RestirGiReservoirs, RestirLightsDesc, RestirMeshDesc,
                   RestirParams, RestirScene, RestirSettings)
 
-LIBRARY_PATH = Path(__file__).resolve().parent / "librestir_gpu.so"
+# RESTIR_LIBRARY selects another build of the same library (tuning variants).
+LIBRARY_PATH = Path(os.environ.get("RESTIR_LIBRARY", Path(__file__).resolve().parent / "librestir_gpu.so"))
 
 SCENE_CORNELL, SCENE_COURTYARD, SCENE_CITY = 0, 1, 2
 GRID_ATOMIC, GRID_DETERMINISTIC = 0, 1

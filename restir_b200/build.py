@@ -56,19 +56,25 @@ def _run(command: list[str]) -> None:
         raise RuntimeError("build failed:\n" + " ".join(command) + "\n" + result.stdout + result.stderr)
 
 
-def build(verbose: bool = False) -> Path:
-    BUILD.mkdir(exist_ok=True)
+def build(verbose: bool = False, defines: list[str] | None = None, library: Path = LIBRARY,
+          objects_dir: Path = BUILD) -> Path:
+    """Compiles stale objects and links the library. defines: extra -D macros for
+    the CUDA sources (tuning knobs such as RESTIR_GI_TEMPORAL_MIN_BLOCKS=4),
+    built into their own objects_dir and library."""
+    objects_dir = Path(objects_dir)
+    objects_dir.mkdir(parents=True, exist_ok=True)
     nvcc = _nvcc()
     headers = _headers()
+    extra = [f"-D{d}" for d in (defines or [])]
     jobs = []
     objects = []
     for source in sorted(CSRC.glob("*.cu")):
-        obj = BUILD / (source.stem + ".cu.o")
+        obj = objects_dir / (source.stem + ".cu.o")
         objects.append(obj)
         if _stale(obj, [source] + headers):
-            jobs.append([nvcc] + NVCC_FLAGS + ["-c", str(source), "-o", str(obj)])
+            jobs.append([nvcc] + NVCC_FLAGS + extra + ["-c", str(source), "-o", str(obj)])
     for source in sorted(HOST.glob("*.cpp")):
-        obj = BUILD / (source.stem + ".cpp.o")
+        obj = objects_dir / (source.stem + ".cpp.o")
         objects.append(obj)
         if _stale(obj, [source] + headers):
             jobs.append(["g++"] + CXX_FLAGS + ["-c", str(source), "-o", str(obj)])
@@ -77,10 +83,12 @@ def build(verbose: bool = False) -> Path:
             if verbose:
                 print(" ".join(command), file=sys.stderr)
         list(pool.map(_run, jobs))
-    if jobs or _stale(LIBRARY, objects):
+    library = Path(library)
+    library.parent.mkdir(parents=True, exist_ok=True)
+    if jobs or _stale(library, objects):
         _run([nvcc] + ARCH + ["-shared", "-rdc=true", "-Xcompiler", "-fPIC"] + [str(o) for o in objects]
-             + ["-o", str(LIBRARY), "-lcudart"])
-    return LIBRARY
+             + ["-o", str(library), "-lcudart"])
+    return library
 
 
 if __name__ == "__main__":

@@ -6,6 +6,17 @@
 #include "bvh.cuh"
 #include "screen.cuh"
 
+// Minimum resident blocks per SM (register budget) of the two DI kernels:
+// 8 blocks of 128 threads (64 registers) measured fastest on the 1080p
+// frame; the shadow rays are latency-bound, so more warps in flight win
+// over the few registers spilled to L1.
+#ifndef RESTIR_DI_TEMPORAL_MIN_BLOCKS
+#	define RESTIR_DI_TEMPORAL_MIN_BLOCKS 8
+#endif
+#ifndef RESTIR_DI_SPATIAL_MIN_BLOCKS
+#	define RESTIR_DI_SPATIAL_MIN_BLOCKS 8
+#endif
+
 namespace restir
 {
 namespace
@@ -208,7 +219,7 @@ __device__ __forceinline__ DiPass makeDiPass(const RestirParams& P, const BvhVie
 	return d;
 }
 
-__global__ void __launch_bounds__(128) diTemporalKernel(const RestirParams P, BvhView bvh, const float* lights, RestirGBuffer gb,
+__global__ void __launch_bounds__(128, RESTIR_DI_TEMPORAL_MIN_BLOCKS) diTemporalKernel(const RestirParams P, BvhView bvh, const float* lights, RestirGBuffer gb,
 	RestirDiReservoirs previous, RestirDiReservoirs out)
 {
 	const int px = int(blockIdx.x * 16 + threadIdx.x % 16);
@@ -338,7 +349,7 @@ __global__ void __launch_bounds__(128) diTemporalKernel(const RestirParams P, Bv
 	storeH4(out.normal, i, v4(surface.normal, canonicalCount + temporalCount));
 }
 
-__global__ void __launch_bounds__(128) diSpatialKernel(const RestirParams P, BvhView bvh, const float* lights, RestirGBuffer gb,
+__global__ void __launch_bounds__(128, RESTIR_DI_SPATIAL_MIN_BLOCKS) diSpatialKernel(const RestirParams P, BvhView bvh, const float* lights, RestirGBuffer gb,
 	RestirDiReservoirs current, uint16_t* diffuseOut, uint16_t* specularOut)
 {
 	const int px = int(blockIdx.x * 16 + threadIdx.x % 16);

@@ -16,6 +16,17 @@ namespace
 constexpr int kGiWarps = 4;
 constexpr int kGiThreads = 32 * kGiWarps;
 
+// Minimum resident blocks per SM (register budget) of the two GI kernels.
+// Measured on the 1080p frame (launch-bound sweep): the spatial pass gains
+// from 8 blocks (64 registers, a little spilling to L1); the temporal pass is
+// bound by divergence, not occupancy, and keeps its registers.
+#ifndef RESTIR_GI_TEMPORAL_MIN_BLOCKS
+#	define RESTIR_GI_TEMPORAL_MIN_BLOCKS 1
+#endif
+#ifndef RESTIR_GI_SPATIAL_MIN_BLOCKS
+#	define RESTIR_GI_SPATIAL_MIN_BLOCKS 8
+#endif
+
 struct GiBindings
 {
 	const uint8_t* albedo;
@@ -69,7 +80,8 @@ __device__ __forceinline__ V4 f4(float4 q)
 	return { q.x, q.y, q.z, q.w };
 }
 
-__global__ void __launch_bounds__(kGiThreads) giTemporalKernel(const RestirParams P, BvhView bvh, GiBindings b)
+__global__ void __launch_bounds__(kGiThreads, RESTIR_GI_TEMPORAL_MIN_BLOCKS) giTemporalKernel(const RestirParams P, BvhView bvh,
+	GiBindings b)
 {
 	__shared__ int stackStorage[kBvhShortStack * kGiThreads];
 	const int lane = int(threadIdx.x & 31u);
@@ -258,7 +270,7 @@ __global__ void __launch_bounds__(kGiThreads) giTemporalKernel(const RestirParam
 	}
 }
 
-__global__ void __launch_bounds__(128) giSpatialKernel(const RestirParams P, BvhView bvh, GiBindings b)
+__global__ void __launch_bounds__(128, RESTIR_GI_SPATIAL_MIN_BLOCKS) giSpatialKernel(const RestirParams P, BvhView bvh, GiBindings b)
 {
 	const int px = int(blockIdx.x * 16 + threadIdx.x % 16);
 	const int py = int(blockIdx.y * 8 + threadIdx.x / 16);
