@@ -61,6 +61,8 @@ typedef struct RestirSettings
 	uint32_t grid_table_size;
 	uint32_t grid_cell_capacity;
 	uint32_t grid_mode;      /* RESTIR_GRID_* */
+	uint32_t wavefront;      /* no reference counterpart: 1 runs the GI temporal pass as
+	                            restir_gi_temporal_wavefront (same output), 0 as restir_gi_temporal */
 } RestirSettings;
 
 /* FrameInput (renderer.h) with the fly camera's pose. */

@@ -63,6 +63,9 @@ extern "C" {
 #define RESTIR_TRACE_ANY 1               /* stackless, first hit (bvh.sh:140-174) */
 #define RESTIR_TRACE_CLOSEST_STACKLESS 2 /* stackless, nearest hit (bvh.sh:140-174) */
 #define RESTIR_TRACE_CLOSEST_WATERTIGHT 3 /* full stack, watertight triangle test */
+#define RESTIR_TRACE_CLOSEST_QUEUE 4     /* RESTIR_TRACE_CLOSEST through the persistent
+                                            queue tracer (same results; no reference
+                                            counterpart) */
 
 /*
  * Everything the reference passes read from vec4 uniforms, by name. Values
@@ -236,6 +239,24 @@ int restir_gi_temporal(const RestirParams* params, const RestirScene* scene, con
 	const RestirGiHistory* history, const uint32_t* previous_grid, const float* shadow_atlas,
 	const uint16_t* surface_light, const RestirGiReservoirs* output, void* stream);
 
+/* No reference counterpart: the bytes of device workspace that
+ * restir_gi_temporal_wavefront needs for these params (60 bytes per GI
+ * pixel and initial candidate, in six regions each rounded up to 256). */
+uint64_t restir_gi_temporal_workspace_bytes(const RestirParams* params);
+
+/* restir_gi_temporal as a wavefront, with identical outputs: a candidates
+ * pass (directions and depth-buffer marches) appends the rays it cannot
+ * answer to a queue in the workspace, a persistent tracer walks the queue
+ * (a lane takes the next ray as soon as its own finishes), and a shading
+ * pass completes cs_restir_temporal.sc from the recorded hits. workspace:
+ * 256-byte aligned device memory of at least
+ * restir_gi_temporal_workspace_bytes; it must not be shared with a call
+ * whose kernels may overlap this one's. */
+int restir_gi_temporal_wavefront(const RestirParams* params, const RestirScene* scene, const RestirGBuffer* gbuffer,
+	const RestirGiHistory* history, const uint32_t* previous_grid, const float* shadow_atlas,
+	const uint16_t* surface_light, const RestirGiReservoirs* output, void* workspace, uint64_t workspace_bytes,
+	void* stream);
+
 /* color, moments: half4 at GI resolution. */
 int restir_gi_spatial(const RestirParams* params, const RestirScene* scene, const RestirGBuffer* gbuffer,
 	const RestirGiReservoirs* current, const uint32_t* current_grid, const RestirGiHistory* history,
@@ -295,7 +316,8 @@ int restir_error_noalloc(const RestirParams* params, const uint16_t* display, co
 	const uint8_t* alpha, double* out, void* stream);
 
 /* Reads and clears the device status word: bit 0 a traversal reached its
- * step cap, bit 1 a hash grid probe sequence was exhausted. */
+ * step cap, bit 1 a hash grid probe sequence was exhausted, bit 2 a ray
+ * queue was full (rays past its capacity are not traced). */
 int restir_status(uint32_t* flags);
 
 /* Work counters: waits for the device, returns the counts gathered since the

@@ -44,9 +44,13 @@ LAYOUT = {
 
 
 class FrameRunner:
-    def __init__(self, setup, width: int, height: int, backend: str = "oracle", settings=None):
+    def __init__(self, setup, width: int, height: int, backend: str = "oracle", settings=None,
+                 gi_wavefront: bool = False):
         self.setup = setup
         self.backend = backend
+        # cuda backend: the GI temporal pass through restir_gi_temporal_wavefront
+        self.gi_wavefront = gi_wavefront and backend == "cuda"
+        self.gi_workspace = None
         self.settings = settings or setup.settings
         self.width, self.height = width, height
         self.state = rb.initial_state()
@@ -124,8 +128,12 @@ class FrameRunner:
         history = RestirGiHistory(self.b(f"gi.sample{hr}"), self.b(f"gi.receiver{hr}"), self.b(f"gi.normal{hr}"),
                                   color_read, self.b(f"gi.moments{hr}"))
         current = RestirGiReservoirs(self.b(f"gi.sample{hw}"), self.b(f"gi.receiver{hw}"), self.b(f"gi.normal{hw}"))
-        out.append(("gi_temporal", lambda: self.call("gi_temporal", P, self.scene, gb, history, self.b(f"grid{hr}"),
-                                                     self.b("atlas"), surface, current)))
+        if self.gi_wavefront:
+            out.append(("gi_temporal", lambda: self.gi_temporal_wavefront(P, gb, history, self.b(f"grid{hr}"), surface,
+                                                                          current)))
+        else:
+            out.append(("gi_temporal", lambda: self.call("gi_temporal", P, self.scene, gb, history,
+                                                         self.b(f"grid{hr}"), self.b("atlas"), surface, current)))
         out.append(("gi_spatial", lambda: self.call("gi_spatial", P, self.scene, gb, current, self.b(f"grid{hw}"),
                                                     history, self.b("atlas"), surface, self.b(f"gi.color{hw}"),
                                                     self.b(f"gi.moments{hw}"))))
@@ -150,6 +158,16 @@ class FrameRunner:
                 "reference_accumulate", P, self.b("hdr"), self.b("ref.mean"), self.b("ref.alpha"),
                 plan.reference_weight_frames)))
         return out
+
+    def gi_temporal_wavefront(self, P, gb, history, grid, surface, current):
+        import torch
+        nbytes = int(self.lib.restir_gi_temporal_workspace_bytes(P))
+        if self.gi_workspace is None or self.gi_workspace.numel() < nbytes:
+            self.gi_workspace = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+        assert self.gi_workspace.data_ptr() % 256 == 0
+        rb.check(self.lib.restir_gi_temporal_wavefront(P, self.scene, gb, history, grid, self.b("atlas"), surface,
+                                                        current, self.gi_workspace.data_ptr(), nbytes, None),
+                 "gi_temporal_wavefront")
 
     def finish(self):
         rb.advance(self.params, self.plan, self.frame_input, self.state)
@@ -199,12 +217,12 @@ class FrameRunner:
 
 
 def run_checked(setup, width: int, height: int, frames: int, settings=None, on_mismatch=None,
-                reference_frames: int = 0):
+                reference_frames: int = 0, gi_wavefront: bool = False):
     """Runs `frames` frames on both backends, feeding each CUDA pass the oracle's
     inputs and comparing its outputs bit for bit. Returns {pass: mismatching elements}."""
     import torch
     oracle_run = FrameRunner(setup, width, height, "oracle", settings)
-    cuda_run = FrameRunner(setup, width, height, "cuda", settings)
+    cuda_run = FrameRunner(setup, width, height, "cuda", settings, gi_wavefront=gi_wavefront)
     report = {}
     for frame in range(frames):
         if reference_frames and frame == frames - reference_frames:

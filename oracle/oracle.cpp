@@ -20,7 +20,8 @@
  *                                back-face discard) at pixel centres
  *   oracle_shadow_atlas          shaders/fs_shadow.sc:13-23 at texel centres
  * Pixels are independent except where the shader shares a group (the GI
- * temporal pass's 4x8 group sum), and are spread over OpenMP threads.
+ * temporal pass's 4x8 group sum), and are spread over std::thread workers
+ * (parallel.h).
  */
 #include "oracle.h"
 #include "oracle_gi.h"
@@ -119,39 +120,39 @@ extern "C" int oracle_trace(const RestirParams* params, const RestirScene* scene
 	(void)params;
 	resetCounts();
 	Bvh base = makeBvh(scene);
-const int threadCount = threads();
-	std::vector<Bvh> bs_(size_t(threadCount), base);
-	parallelFor(int64_t(int64_t(n)), 256, [&](int64_t i_, int thread_)
+	const int threadCount = threads();
+	std::vector<Bvh> perThread(size_t(threadCount), base);
+	parallelFor(int64_t(n), 256, [&](int64_t i, int thread)
 	{
-		Bvh& b = bs_[size_t(thread_)];
-		int64_t i = int64_t(i_);
-			const float* r = rays + 8 * i;
-			vec3 origin(r[0], r[1], r[2]);
-			vec3 direction(r[4], r[5], r[6]);
-			float distance_ = r[3];
-			int hit = -1;
-			if (kind == RESTIR_TRACE_CLOSEST)
-			{
-				hit = traceBvh(b, origin, direction, r[3], false, distance_, true);
-			}
-			else if (kind == RESTIR_TRACE_ANY)
-			{
-				hit = traceBvh(b, origin, direction, r[3], true, distance_, false);
-			}
-			else if (kind == RESTIR_TRACE_CLOSEST_STACKLESS)
-			{
-				hit = traceBvh(b, origin, direction, r[3], false, distance_, false);
-			}
-			else
-			{
-				hit = b.available() ? traceWatertight(b, origin, direction, distance_) : -1;
-			}
-			hit_triangle[i] = hit;
-			hit_distance[i] = distance_;
-		});
-	for (int t_ = 0; t_ < threadCount; ++t_)
+		Bvh& b = perThread[size_t(thread)];
+		const float* r = rays + 8 * i;
+		vec3 origin(r[0], r[1], r[2]);
+		vec3 direction(r[4], r[5], r[6]);
+		float distance = r[3];
+		int hit = -1;
+		// The queued closest-hit kind differs only in scheduling.
+		if (kind == RESTIR_TRACE_CLOSEST || kind == RESTIR_TRACE_CLOSEST_QUEUE)
+		{
+			hit = traceBvh(b, origin, direction, r[3], false, distance, true);
+		}
+		else if (kind == RESTIR_TRACE_ANY)
+		{
+			hit = traceBvh(b, origin, direction, r[3], true, distance, false);
+		}
+		else if (kind == RESTIR_TRACE_CLOSEST_STACKLESS)
+		{
+			hit = traceBvh(b, origin, direction, r[3], false, distance, false);
+		}
+		else
+		{
+			hit = b.available() ? traceWatertight(b, origin, direction, distance) : -1;
+		}
+		hit_triangle[i] = hit;
+		hit_distance[i] = distance;
+	});
+	for (int t = 0; t < threadCount; ++t)
 	{
-		addCounts(bs_[size_t(t_)], 0, 0);
+		addCounts(perThread[size_t(t)], 0, 0);
 	}
 	return RESTIR_OK;
 }

@@ -29,7 +29,10 @@ LIBRARY_PATH = Path(os.environ.get("RESTIR_LIBRARY", Path(__file__).resolve().pa
 SCENE_CORNELL, SCENE_COURTYARD, SCENE_CITY = 0, 1, 2
 GRID_ATOMIC, GRID_DETERMINISTIC = 0, 1
 RAY_SCREEN, RAY_HYBRID, RAY_BVH = 0, 1, 2
-TRACE_CLOSEST, TRACE_ANY, TRACE_CLOSEST_STACKLESS, TRACE_CLOSEST_WATERTIGHT = 0, 1, 2, 3
+# restir_gpu.h status codes
+OK, ERROR_INVALID_ARGUMENT, ERROR_LAUNCH, ERROR_STEP_CAP, ERROR_UNSUPPORTED = 0, -1, -2, -3, -4
+ERROR_TIMEOUT, ERROR_OUT_OF_MEMORY, ERROR_TOO_LARGE = -5, -6, -7
+TRACE_CLOSEST, TRACE_ANY, TRACE_CLOSEST_STACKLESS, TRACE_CLOSEST_WATERTIGHT, TRACE_CLOSEST_QUEUE = 0, 1, 2, 3, 4
 PASS_NAMES = ["shadow", "gbuffer", "di_temporal", "di_spatial", "grid", "gi_temporal", "gi_spatial",
               "denoise", "composite", "reference"]
 
@@ -52,6 +55,10 @@ _SIGNATURES = {
                                     C.POINTER(RestirDiReservoirs), P, P, P]),
     "restir_gi_temporal": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirScene), C.POINTER(RestirGBuffer),
                                      C.POINTER(RestirGiHistory), P, P, P, C.POINTER(RestirGiReservoirs), P]),
+    "restir_gi_temporal_workspace_bytes": (C.c_uint64, [C.POINTER(RestirParams)]),
+    "restir_gi_temporal_wavefront": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirScene),
+                                               C.POINTER(RestirGBuffer), C.POINTER(RestirGiHistory), P, P, P,
+                                               C.POINTER(RestirGiReservoirs), P, C.c_uint64, P]),
     "restir_gi_spatial": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirScene), C.POINTER(RestirGBuffer),
                                     C.POINTER(RestirGiReservoirs), P, C.POINTER(RestirGiHistory), P, P, P, P, P]),
     "restir_svgf_variance": (C.c_int, [C.POINTER(RestirParams), P, P, P, P, P, P]),
@@ -60,6 +67,7 @@ _SIGNATURES = {
     "restir_reference_accumulate": (C.c_int, [C.POINTER(RestirParams), P, P, P, u32, P]),
     "restir_error_scratch_bytes": (C.c_uint64, [u32, u32]),
     "restir_error": (C.c_int, [C.POINTER(RestirParams), P, P, P, P, P, P]),
+    "restir_error_noalloc": (C.c_int, [C.POINTER(RestirParams), P, P, P, P, P]),
     "restir_status": (C.c_int, [C.POINTER(u32)]),
     "restir_numeric_eval": (C.c_int, [C.c_int, P, P, u32, P]),
     "restir_counters": (C.c_int, [C.c_int, P]),
@@ -102,11 +110,6 @@ _SIGNATURES = {
     "restir_renderer_buffer": (C.c_int, [P, C.c_char_p, C.POINTER(P), C.POINTER(C.c_uint64)]),
 }
 
-# Entry points that may be absent while the library is being extended.
-_OPTIONAL = {"restir_di_temporal", "restir_di_spatial", "restir_gi_temporal", "restir_gi_spatial",
-             "restir_svgf_variance", "restir_svgf_atrous", "restir_composite", "restir_reference_accumulate",
-             "restir_error_scratch_bytes", "restir_error"}
-
 
 def load() -> C.CDLL:
     """The CUDA library. Raises if it has not been built (python -m restir_b200.build)."""
@@ -117,8 +120,6 @@ def load() -> C.CDLL:
         lib = C.CDLL(str(LIBRARY_PATH))
         for name, (restype, argtypes) in _SIGNATURES.items():
             if not hasattr(lib, name):
-                if name in _OPTIONAL:
-                    continue
                 raise RuntimeError(f"{LIBRARY_PATH} does not export {name}")
             fn = getattr(lib, name)
             fn.restype = restype

@@ -101,6 +101,7 @@ class RestirSettings(C.Structure):
         ("initial_candidates", C.c_int), ("temporal_taps", C.c_int), ("spatial_taps", C.c_int),
         ("trace_steps", C.c_int), ("di_candidates", C.c_int), ("di_spatial_taps", C.c_int),
         ("grid_table_size", C.c_uint32), ("grid_cell_capacity", C.c_uint32), ("grid_mode", C.c_uint32),
+        ("wavefront", C.c_uint32),
     ]
 
 

@@ -7,6 +7,7 @@
 // and closest-hit candidate rays keep their short traversal stack in shared
 // memory, interleaved across the block's lanes.
 #include "gi.cuh"
+#include "wavefront.cuh"
 
 namespace restir
 {
@@ -80,97 +81,12 @@ __device__ __forceinline__ V4 f4(float4 q)
 	return { q.x, q.y, q.z, q.w };
 }
 
-__global__ void __launch_bounds__(kGiThreads, RESTIR_GI_TEMPORAL_MIN_BLOCKS) giTemporalKernel(const RestirParams P, BvhView bvh,
-	GiBindings b)
+// cs_restir_temporal.sc:192-296 after the fresh candidates: temporal reuse
+// with pairwise MIS, the boiling filter over the warp's 4x8 group, the
+// reservoir stores. Every lane of the warp must call it (the group sum).
+__device__ __forceinline__ void temporalReuseAndStore(const RestirParams& P, const GiPass& g, const GiBindings& b, int lane,
+	bool inside, bool working, int px, int py, V3 position, V3 normal, V3 albedo, const GiReservoir& canonical, uint32_t rng)
 {
-	__shared__ int stackStorage[kBvhShortStack * kGiThreads];
-	const int lane = int(threadIdx.x & 31u);
-	const int groupsX = (int(P.gi_width) + 3) / 4;
-	const int groupsY = (int(P.gi_height) + 7) / 8;
-	const int group = int(blockIdx.x) * kGiWarps + int(threadIdx.x >> 5);
-	if (group >= groupsX * groupsY)
-	{
-		return; // whole warp
-	}
-	GiPass g = makePass(P, bvh, b, P.prev_camera_position, stackStorage + threadIdx.x, kGiThreads);
-	const int px = (group % groupsX) * 4 + (lane & 3);
-	const int py = (group / groupsX) * 8 + (lane >> 2);
-	const bool inside = px < g.w && py < g.h;
-	const V2 uv = pixelUv(px, py, g.giTexel);
-	const float depth = inside ? g.depthAt(uv) : 1.0f;
-	const bool working = inside && depth < kSkyDepth;
-
-	const V3 position = reconstructWorldPosition(P, uv, depth);
-	const V3 normal = g.decode(uv);
-	const V3 albedo = g.diffuseAlbedo(uv);
-	const V3 rayOrigin = position + normal * g.kRayBias();
-	const V2 giPixelCoord = v2(floorf(uv.x * g.giSize.x), floorf(uv.y * g.giSize.y));
-	uint32_t rng = pcg(uint32_t(giPixelCoord.x) + pcg(uint32_t(giPixelCoord.y) + pcg(uint32_t(P.frame_index))));
-
-	GiReservoir canonical = emptyReservoir();
-	for (int sampleIndex = 0; sampleIndex < P.initial_candidates; ++sampleIndex)
-	{
-		float random0 = nextRandom(rng);
-		float random1 = nextRandom(rng);
-		float randomSelect = nextRandom(rng);
-		V3 direction = GiPass::cosineHemisphere(normal, random0, random1);
-		canonical.count += 1.0f;
-		V3 hitPosition = v3s(0.0f);
-		float hitId = 0.0f;
-		bool hit = false;
-		if (working && P.ray_mode != RESTIR_RAY_MODE_BVH)
-		{
-			hit = g.traceScreenSpaceRay(rayOrigin, direction, g.kMaxRayDistance(), hitPosition);
-		}
-		bool needBvh = working && !hit && P.ray_mode != RESTIR_RAY_MODE_SCREEN;
-		if (needBvh)
-		{
-			float queueDistance;
-			int queueTriangle = traceBvh(g.bvh, rayOrigin, direction, g.kMaxBvhRayDistance(), false, queueDistance,
-				g.stack, g.stackStride);
-			if (queueTriangle >= 0)
-			{
-				hit = true;
-				hitPosition = rayOrigin + direction * queueDistance;
-				hitId = g.encodeSampleId(queueTriangle, direction);
-			}
-			else if (skyEnabled(P))
-			{
-				hit = true;
-				hitPosition = direction;
-				hitId = kSkySampleId;
-			}
-		}
-		V3 contribution = v3s(0.0f);
-		V3 hitNormal = v3s(0.0f);
-		bool evaluated = false;
-		if (hit)
-		{
-			evaluated = g.evaluateSample(position, normal, albedo, hitPosition, hitId, contribution, hitNormal);
-		}
-		if (evaluated)
-		{
-			float target = luminance(contribution);
-			float sourcePdf = dot(normal, direction) / kPi;
-			if (!isSkySample(hitId))
-			{
-				V3 fromReceiver = hitPosition - position;
-				V3 fromOrigin = hitPosition - rayOrigin;
-				float receiverSquared = fmaxf(dot(fromReceiver, fromReceiver), g.kMinDistanceSquared() * 0.01f);
-				float originSquared = fmaxf(dot(fromOrigin, fromOrigin), g.kMinDistanceSquared() * 0.01f);
-				float hitCosineOrigin = fmaxf(-dot(hitNormal, fromOrigin), 0.0f) * inversesqrt(originSquared);
-				float hitCosineReceiver = -dot(hitNormal, fromReceiver) * inversesqrt(receiverSquared);
-				sourcePdf = hitCosineReceiver > 0.0001f
-					? sourcePdf * (hitCosineOrigin / originSquared) * (receiverSquared / hitCosineReceiver)
-					: 0.0f;
-			}
-			if (target > 0.0f && sourcePdf > 0.0001f)
-			{
-				updateReservoir(canonical, contribution, hitPosition, hitNormal, hitId, target, target / sourcePdf, randomSelect);
-			}
-		}
-	}
-
 	const float canonicalWeight = canonical.target > 0.000001f ? canonical.weightSum / (canonical.count * canonical.target) : 0.0f;
 	const bool historyValid = P.history_valid > 0.5f;
 	V2 previousUv = v2(0.0f, 0.0f);
@@ -268,6 +184,100 @@ __global__ void __launch_bounds__(kGiThreads, RESTIR_GI_TEMPORAL_MIN_BLOCKS) giT
 			: make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 		b.outNormal[i] = working ? make_float4(normal.x, normal.y, normal.z, mis.combined.id) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 	}
+}
+
+__global__ void __launch_bounds__(kGiThreads, RESTIR_GI_TEMPORAL_MIN_BLOCKS) giTemporalKernel(const RestirParams P, BvhView bvh,
+	GiBindings b)
+{
+	__shared__ int stackStorage[kBvhShortStack * kGiThreads];
+	const int lane = int(threadIdx.x & 31u);
+	const int groupsX = (int(P.gi_width) + 3) / 4;
+	const int groupsY = (int(P.gi_height) + 7) / 8;
+	const int group = int(blockIdx.x) * kGiWarps + int(threadIdx.x >> 5);
+	if (group >= groupsX * groupsY)
+	{
+		return; // whole warp
+	}
+	GiPass g = makePass(P, bvh, b, P.prev_camera_position, stackStorage + threadIdx.x, kGiThreads);
+	const int px = (group % groupsX) * 4 + (lane & 3);
+	const int py = (group / groupsX) * 8 + (lane >> 2);
+	const bool inside = px < g.w && py < g.h;
+	const V2 uv = pixelUv(px, py, g.giTexel);
+	const float depth = inside ? g.depthAt(uv) : 1.0f;
+	const bool working = inside && depth < kSkyDepth;
+
+	const V3 position = reconstructWorldPosition(P, uv, depth);
+	const V3 normal = g.decode(uv);
+	const V3 albedo = g.diffuseAlbedo(uv);
+	const V3 rayOrigin = position + normal * g.kRayBias();
+	const V2 giPixelCoord = v2(floorf(uv.x * g.giSize.x), floorf(uv.y * g.giSize.y));
+	uint32_t rng = pcg(uint32_t(giPixelCoord.x) + pcg(uint32_t(giPixelCoord.y) + pcg(uint32_t(P.frame_index))));
+
+	GiReservoir canonical = emptyReservoir();
+	for (int sampleIndex = 0; sampleIndex < P.initial_candidates; ++sampleIndex)
+	{
+		float random0 = nextRandom(rng);
+		float random1 = nextRandom(rng);
+		float randomSelect = nextRandom(rng);
+		V3 direction = GiPass::cosineHemisphere(normal, random0, random1);
+		canonical.count += 1.0f;
+		V3 hitPosition = v3s(0.0f);
+		float hitId = 0.0f;
+		bool hit = false;
+		if (working && P.ray_mode != RESTIR_RAY_MODE_BVH)
+		{
+			hit = g.traceScreenSpaceRay(rayOrigin, direction, g.kMaxRayDistance(), hitPosition);
+		}
+		bool needBvh = working && !hit && P.ray_mode != RESTIR_RAY_MODE_SCREEN;
+		if (needBvh)
+		{
+			float queueDistance;
+			int queueTriangle = traceBvh(g.bvh, rayOrigin, direction, g.kMaxBvhRayDistance(), false, queueDistance,
+				g.stack, g.stackStride);
+			if (queueTriangle >= 0)
+			{
+				hit = true;
+				hitPosition = rayOrigin + direction * queueDistance;
+				hitId = g.encodeSampleId(queueTriangle, direction);
+			}
+			else if (skyEnabled(P))
+			{
+				hit = true;
+				hitPosition = direction;
+				hitId = kSkySampleId;
+			}
+		}
+		V3 contribution = v3s(0.0f);
+		V3 hitNormal = v3s(0.0f);
+		bool evaluated = false;
+		if (hit)
+		{
+			evaluated = g.evaluateSample(position, normal, albedo, hitPosition, hitId, contribution, hitNormal);
+		}
+		if (evaluated)
+		{
+			float target = luminance(contribution);
+			float sourcePdf = dot(normal, direction) / kPi;
+			if (!isSkySample(hitId))
+			{
+				V3 fromReceiver = hitPosition - position;
+				V3 fromOrigin = hitPosition - rayOrigin;
+				float receiverSquared = fmaxf(dot(fromReceiver, fromReceiver), g.kMinDistanceSquared() * 0.01f);
+				float originSquared = fmaxf(dot(fromOrigin, fromOrigin), g.kMinDistanceSquared() * 0.01f);
+				float hitCosineOrigin = fmaxf(-dot(hitNormal, fromOrigin), 0.0f) * inversesqrt(originSquared);
+				float hitCosineReceiver = -dot(hitNormal, fromReceiver) * inversesqrt(receiverSquared);
+				sourcePdf = hitCosineReceiver > 0.0001f
+					? sourcePdf * (hitCosineOrigin / originSquared) * (receiverSquared / hitCosineReceiver)
+					: 0.0f;
+			}
+			if (target > 0.0f && sourcePdf > 0.0001f)
+			{
+				updateReservoir(canonical, contribution, hitPosition, hitNormal, hitId, target, target / sourcePdf, randomSelect);
+			}
+		}
+	}
+
+	temporalReuseAndStore(P, g, b, lane, inside, working, px, py, position, normal, albedo, canonical, rng);
 }
 
 __global__ void __launch_bounds__(128, RESTIR_GI_SPATIAL_MIN_BLOCKS) giSpatialKernel(const RestirParams P, BvhView bvh, GiBindings b)
@@ -425,6 +435,175 @@ __global__ void __launch_bounds__(128, RESTIR_GI_SPATIAL_MIN_BLOCKS) giSpatialKe
 	storeH4(b.outMoments, outIndex, v4(m0, m1, historyLength, 0.0f));
 }
 
+// --- the temporal pass as a wavefront -----------------------------------------
+//
+// A: candidate directions and depth-buffer marches; the rays the march cannot
+//    answer go to a ray queue (warp-vote compaction).
+// B: the persistent closest-hit tracer over the queue (wavefront.cuh).
+// C: the rest of cs_restir_temporal.sc, reading A's and B's results where
+//    the megakernel traced; the random stream is replayed from the pixel's
+//    seed, so every number is the megakernel's.
+
+struct CandidateRecords
+{
+	float4* screenHit;  // per pixel and candidate: (hit position, 1 if the march hit)
+	int* slot;          // per pixel and candidate: queue slot, or -1
+	int candidates;
+};
+
+__global__ void __launch_bounds__(kGiThreads) giCandidatesKernel(const RestirParams P, BvhView bvh, GiBindings b,
+	CandidateRecords records, RayQueue queue)
+{
+	const int lane = int(threadIdx.x & 31u);
+	const int groupsX = (int(P.gi_width) + 3) / 4;
+	const int groupsY = (int(P.gi_height) + 7) / 8;
+	const int group = int(blockIdx.x) * kGiWarps + int(threadIdx.x >> 5);
+	if (group >= groupsX * groupsY)
+	{
+		return; // whole warp
+	}
+	GiPass g = makePass(P, bvh, b, P.prev_camera_position, nullptr, 0);
+	const int px = (group % groupsX) * 4 + (lane & 3);
+	const int py = (group / groupsX) * 8 + (lane >> 2);
+	const bool inside = px < g.w && py < g.h;
+	const V2 uv = pixelUv(px, py, g.giTexel);
+	const float depth = inside ? g.depthAt(uv) : 1.0f;
+	const bool working = inside && depth < kSkyDepth;
+	const V3 position = reconstructWorldPosition(P, uv, depth);
+	const V3 normal = g.decode(uv);
+	const V3 rayOrigin = position + normal * g.kRayBias();
+	const V2 giPixelCoord = v2(floorf(uv.x * g.giSize.x), floorf(uv.y * g.giSize.y));
+	uint32_t rng = pcg(uint32_t(giPixelCoord.x) + pcg(uint32_t(giPixelCoord.y) + pcg(uint32_t(P.frame_index))));
+	const int pixel = py * g.w + px;
+	for (int sampleIndex = 0; sampleIndex < P.initial_candidates; ++sampleIndex)
+	{
+		float random0 = nextRandom(rng);
+		float random1 = nextRandom(rng);
+		nextRandom(rng); // randomSelect, used by pass C
+		V3 direction = GiPass::cosineHemisphere(normal, random0, random1);
+		V3 hitPosition = v3s(0.0f);
+		bool hit = false;
+		if (working && P.ray_mode != RESTIR_RAY_MODE_BVH)
+		{
+			hit = g.traceScreenSpaceRay(rayOrigin, direction, g.kMaxRayDistance(), hitPosition);
+		}
+		const bool needBvh = working && !hit && P.ray_mode != RESTIR_RAY_MODE_SCREEN && bvh.available();
+		const int slot = queuePush(queue, needBvh, rayOrigin, g.kMaxBvhRayDistance(), direction);
+		if (inside)
+		{
+			const int r = pixel * records.candidates + sampleIndex;
+			records.screenHit[r] = make_float4(hitPosition.x, hitPosition.y, hitPosition.z, hit ? 1.0f : 0.0f);
+			records.slot[r] = needBvh ? slot : -2 - int(working && !hit && P.ray_mode != RESTIR_RAY_MODE_SCREEN);
+		}
+	}
+}
+
+__global__ void __launch_bounds__(128) traceQueueKernel(BvhView bvh, RayQueue queue)
+{
+	__shared__ int stackStorage[kBvhShortStack * 128];
+	traceQueueClosest<128>(bvh, queue, stackStorage);
+}
+
+__global__ void __launch_bounds__(kGiThreads, RESTIR_GI_TEMPORAL_MIN_BLOCKS) giTemporalShadeKernel(const RestirParams P,
+	BvhView bvh, GiBindings b, CandidateRecords records, RayQueue queue)
+{
+	const int lane = int(threadIdx.x & 31u);
+	const int groupsX = (int(P.gi_width) + 3) / 4;
+	const int groupsY = (int(P.gi_height) + 7) / 8;
+	const int group = int(blockIdx.x) * kGiWarps + int(threadIdx.x >> 5);
+	if (group >= groupsX * groupsY)
+	{
+		return; // whole warp
+	}
+	GiPass g = makePass(P, bvh, b, P.prev_camera_position, nullptr, 0);
+	const int px = (group % groupsX) * 4 + (lane & 3);
+	const int py = (group / groupsX) * 8 + (lane >> 2);
+	const bool inside = px < g.w && py < g.h;
+	const V2 uv = pixelUv(px, py, g.giTexel);
+	const float depth = inside ? g.depthAt(uv) : 1.0f;
+	const bool working = inside && depth < kSkyDepth;
+	const V3 position = reconstructWorldPosition(P, uv, depth);
+	const V3 normal = g.decode(uv);
+	const V3 albedo = g.diffuseAlbedo(uv);
+	const V3 rayOrigin = position + normal * g.kRayBias();
+	const V2 giPixelCoord = v2(floorf(uv.x * g.giSize.x), floorf(uv.y * g.giSize.y));
+	uint32_t rng = pcg(uint32_t(giPixelCoord.x) + pcg(uint32_t(giPixelCoord.y) + pcg(uint32_t(P.frame_index))));
+	const int pixel = py * g.w + px;
+
+	GiReservoir canonical = emptyReservoir();
+	for (int sampleIndex = 0; sampleIndex < P.initial_candidates; ++sampleIndex)
+	{
+		float random0 = nextRandom(rng);
+		float random1 = nextRandom(rng);
+		float randomSelect = nextRandom(rng);
+		V3 direction = GiPass::cosineHemisphere(normal, random0, random1);
+		canonical.count += 1.0f;
+		V3 hitPosition = v3s(0.0f);
+		float hitId = 0.0f;
+		bool hit = false;
+		if (inside)
+		{
+			const int r = pixel * records.candidates + sampleIndex;
+			const float4 screen = records.screenHit[r];
+			hit = screen.w > 0.5f;
+			hitPosition = v3(screen.x, screen.y, screen.z);
+			const int slot = records.slot[r];
+			// -3: the BVH was wanted but there is none (traceBvh returns -1 at once).
+			if (slot >= 0 || slot == -3)
+			{
+				int triangle = -1;
+				float t = 0.0f;
+				if (slot >= 0)
+				{
+					triangle = queue.hitTriangle[slot];
+					t = queue.hitDistance[slot];
+				}
+				if (triangle >= 0)
+				{
+					hit = true;
+					hitPosition = rayOrigin + direction * t;
+					hitId = g.encodeSampleId(triangle, direction);
+				}
+				else if (skyEnabled(P))
+				{
+					hit = true;
+					hitPosition = direction;
+					hitId = kSkySampleId;
+				}
+			}
+		}
+		V3 contribution = v3s(0.0f);
+		V3 hitNormal = v3s(0.0f);
+		bool evaluated = false;
+		if (hit)
+		{
+			evaluated = g.evaluateSample(position, normal, albedo, hitPosition, hitId, contribution, hitNormal);
+		}
+		if (evaluated)
+		{
+			float target = luminance(contribution);
+			float sourcePdf = dot(normal, direction) / kPi;
+			if (!isSkySample(hitId))
+			{
+				V3 fromReceiver = hitPosition - position;
+				V3 fromOrigin = hitPosition - rayOrigin;
+				float receiverSquared = fmaxf(dot(fromReceiver, fromReceiver), g.kMinDistanceSquared() * 0.01f);
+				float originSquared = fmaxf(dot(fromOrigin, fromOrigin), g.kMinDistanceSquared() * 0.01f);
+				float hitCosineOrigin = fmaxf(-dot(hitNormal, fromOrigin), 0.0f) * inversesqrt(originSquared);
+				float hitCosineReceiver = -dot(hitNormal, fromReceiver) * inversesqrt(receiverSquared);
+				sourcePdf = hitCosineReceiver > 0.0001f
+					? sourcePdf * (hitCosineOrigin / originSquared) * (receiverSquared / hitCosineReceiver)
+					: 0.0f;
+			}
+			if (target > 0.0f && sourcePdf > 0.0001f)
+			{
+				updateReservoir(canonical, contribution, hitPosition, hitNormal, hitId, target, target / sourcePdf, randomSelect);
+			}
+		}
+	}
+	temporalReuseAndStore(P, g, b, lane, inside, working, px, py, position, normal, albedo, canonical, rng);
+}
+
 GiBindings bindings(const RestirGBuffer* gb, const RestirGiHistory* history, const uint32_t* grid, const float* shadowAtlas,
 	const uint16_t* surfaceLight)
 {
@@ -493,5 +672,104 @@ extern "C" int restir_gi_spatial(const RestirParams* params, const RestirScene* 
 	b.outMoments = moments;
 	dim3 grid((params->gi_width + 15) / 16, (params->gi_height + 7) / 8);
 	giSpatialKernel<<<grid, 128, 0, asStream(stream)>>>(*params, makeBvhView(scene), b);
+	return launchStatus();
+}
+
+namespace
+{
+
+struct TemporalWorkspace
+{
+	RayQueue queue;
+	CandidateRecords records;
+	uint64_t bytes;
+};
+
+// [2 counters][rays 32 B x n][hit triangles 4 B x n][hit distances 4 B x n][screen hits 16 B x n]
+// [slots 4 B x n], each region starting on 256 bytes; n = GI pixels x initial candidates.
+TemporalWorkspace layoutTemporalWorkspace(const RestirParams* p, void* base)
+{
+	const uint64_t n = uint64_t(p->gi_width) * p->gi_height * uint64_t(p->initial_candidates > 0 ? p->initial_candidates : 0);
+	char* at = static_cast<char*>(base);
+	uint64_t offset = 0;
+	auto region = [&](uint64_t bytes) -> char*
+	{
+		char* start = at + offset;
+		offset += (bytes + 255u) & ~uint64_t(255u);
+		return start;
+	};
+	TemporalWorkspace w;
+	uint32_t* counters = reinterpret_cast<uint32_t*>(region(2 * sizeof(uint32_t)));
+	w.queue.count = counters;
+	w.queue.claimed = counters + 1;
+	w.queue.rays = reinterpret_cast<float4*>(region(n * 32));
+	w.queue.hitTriangle = reinterpret_cast<int*>(region(n * 4));
+	w.queue.hitDistance = reinterpret_cast<float*>(region(n * 4));
+	w.records.screenHit = reinterpret_cast<float4*>(region(n * 16));
+	w.records.slot = reinterpret_cast<int*>(region(n * 4));
+	w.queue.capacity = uint32_t(n);
+	w.records.candidates = p->initial_candidates;
+	w.bytes = offset;
+	return w;
+}
+
+// One resident grid of the queue tracer: SMs x blocks that fit on one SM.
+int persistentBlocks()
+{
+	static int blocks = 0;
+	if (blocks == 0)
+	{
+		int device = 0, sms = 148, perSm = 0;
+		if (cudaGetDevice(&device) == cudaSuccess)
+		{
+			cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+		}
+		if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, traceQueueKernel, 128, 0) != cudaSuccess || perSm < 1)
+		{
+			perSm = 1;
+		}
+		blocks = sms * perSm;
+	}
+	return blocks;
+}
+
+} // namespace
+
+extern "C" uint64_t restir_gi_temporal_workspace_bytes(const RestirParams* params)
+{
+	if (params == nullptr)
+	{
+		return 0;
+	}
+	return layoutTemporalWorkspace(params, nullptr).bytes;
+}
+
+extern "C" int restir_gi_temporal_wavefront(const RestirParams* params, const RestirScene* scene, const RestirGBuffer* gbuffer,
+	const RestirGiHistory* history, const uint32_t* previous_grid, const float* shadow_atlas, const uint16_t* surface_light,
+	const RestirGiReservoirs* output, void* workspace, uint64_t workspace_bytes, void* stream)
+{
+	if (!validCommon(params, scene, gbuffer, history, previous_grid, shadow_atlas) || history->sample == nullptr
+		|| output == nullptr || output->sample == nullptr || output->receiver == nullptr || output->normal == nullptr
+		|| workspace == nullptr || (reinterpret_cast<uintptr_t>(workspace) & 255u) != 0u || params->initial_candidates < 0)
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	TemporalWorkspace w = layoutTemporalWorkspace(params, workspace);
+	if (workspace_bytes < w.bytes)
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	GiBindings b = bindings(gbuffer, history, previous_grid, shadow_atlas, surface_light);
+	b.outSample = reinterpret_cast<float4*>(output->sample);
+	b.outReceiver = reinterpret_cast<float4*>(output->receiver);
+	b.outNormal = reinterpret_cast<float4*>(output->normal);
+	const BvhView bvh = makeBvhView(scene);
+	cudaStream_t s = asStream(stream);
+	const int groups = int((params->gi_width + 3) / 4 * ((params->gi_height + 7) / 8));
+	const int blocks = (groups + kGiWarps - 1) / kGiWarps;
+	cudaMemsetAsync(workspace, 0, 2 * sizeof(uint32_t), s);
+	giCandidatesKernel<<<blocks, kGiThreads, 0, s>>>(*params, bvh, b, w.records, w.queue);
+	traceQueueKernel<<<persistentBlocks(), 128, 0, s>>>(bvh, w.queue);
+	giTemporalShadeKernel<<<blocks, kGiThreads, 0, s>>>(*params, bvh, b, w.records, w.queue);
 	return launchStatus();
 }

@@ -1,7 +1,10 @@
 // restir_trace: a fixed ray set through the BVH (bvh.sh:298-319), one thread
 // per ray. Closest-hit rays keep their short stack in shared memory,
 // interleaved so that the 32 lanes of a warp touch 32 different banks.
+// RESTIR_TRACE_CLOSEST_QUEUE runs the same closest-hit traversal through the
+// persistent queue tracer (wavefront.cuh): the ray set is the queue.
 #include "bvh.cuh"
+#include "wavefront.cuh"
 #include "watertight.cuh"
 
 namespace restir
@@ -46,6 +49,26 @@ __global__ void __launch_bounds__(kTraceBlock) traceKernel(BvhView bvh, const fl
 	hitDistance[i] = distance;
 }
 
+__global__ void __launch_bounds__(kTraceBlock) traceQueueKernel(BvhView bvh, RayQueue queue)
+{
+	__shared__ int stack[kBvhShortStack * kTraceBlock];
+	traceQueueClosest<kTraceBlock>(bvh, queue, stack);
+}
+
+int residentQueueBlocks()
+{
+	int device = 0, sms = 148, perSm = 0;
+	if (cudaGetDevice(&device) == cudaSuccess)
+	{
+		cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+	}
+	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, traceQueueKernel, kTraceBlock, 0) != cudaSuccess || perSm < 1)
+	{
+		perSm = 1;
+	}
+	return sms * perSm;
+}
+
 } // namespace
 } // namespace restir
 
@@ -56,7 +79,7 @@ extern "C" int restir_trace(const RestirParams* params, const RestirScene* scene
 {
 	(void)params;
 	if (scene == nullptr || rays == nullptr || hit_triangle == nullptr || hit_distance == nullptr
-		|| kind < RESTIR_TRACE_CLOSEST || kind > RESTIR_TRACE_CLOSEST_WATERTIGHT)
+		|| kind < RESTIR_TRACE_CLOSEST || kind > RESTIR_TRACE_CLOSEST_QUEUE)
 	{
 		return RESTIR_ERROR_INVALID_ARGUMENT;
 	}
@@ -65,7 +88,32 @@ extern "C" int restir_trace(const RestirParams* params, const RestirScene* scene
 		return RESTIR_OK;
 	}
 	BvhView bvh = makeBvhView(scene);
-	traceKernel<<<(n + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, asStream(stream)>>>(
+	cudaStream_t s = asStream(stream);
+	if (kind == RESTIR_TRACE_CLOSEST_QUEUE)
+	{
+		// The claim counter lives in stream-ordered memory, so that calls on
+		// different streams do not share it.
+		uint32_t* claimed = nullptr;
+		if (cudaMallocAsync(reinterpret_cast<void**>(&claimed), sizeof(uint32_t), s) != cudaSuccess)
+		{
+			cudaGetLastError();
+			return RESTIR_ERROR_OUT_OF_MEMORY;
+		}
+		cudaMemsetAsync(claimed, 0, sizeof(uint32_t), s);
+		RayQueue q;
+		q.rays = const_cast<float4*>(reinterpret_cast<const float4*>(rays));
+		q.hitTriangle = hit_triangle;
+		q.hitDistance = hit_distance;
+		q.count = nullptr;
+		q.claimed = claimed;
+		q.capacity = n;
+		static const int blocks = residentQueueBlocks();
+		traceQueueKernel<<<blocks, kTraceBlock, 0, s>>>(bvh, q);
+		const int status = launchStatus();
+		cudaFreeAsync(claimed, s);
+		return status;
+	}
+	traceKernel<<<(n + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, s>>>(
 		bvh, reinterpret_cast<const float4*>(rays), hit_triangle, hit_distance, n, kind);
 	return launchStatus();
 }

@@ -80,6 +80,7 @@ extern "C" void restir_settings_default(RestirSettings* s)
 	s->grid_table_size = 65536;
 	s->grid_cell_capacity = 32;
 	s->grid_mode = RESTIR_GRID_ATOMIC;
+	s->wavefront = 1;
 }
 
 extern "C" int restir_frame_params(const RestirSettings* requested, const RestirMeshDesc* scene, uint32_t light_count,

@@ -147,6 +147,11 @@ public:
 				return status;
 			}
 		}
+		status = ensureWorkspace(m_params);
+		if (status != RESTIR_OK)
+		{
+			return status;
+		}
 		if (graph)
 		{
 			status = renderGraph();
@@ -433,6 +438,33 @@ private:
 		return RESTIR_OK;
 	}
 
+	// The wavefront GI temporal pass's ray queue, sized by the candidate count
+	// (a setting that keeps the history); allocated before any capture.
+	int ensureWorkspace(const RestirParams& P)
+	{
+		const uint64_t needed = m_settings.wavefront ? restir_gi_temporal_workspace_bytes(&P) : 0;
+		auto found = m_targets.find("gi.workspace");
+		if (needed == 0 || (found != m_targets.end() && found->second.bytes >= needed))
+		{
+			return RESTIR_OK;
+		}
+		cudaStreamSynchronize(m_stream);
+		releaseGraph();
+		if (found != m_targets.end())
+		{
+			cudaFree(found->second.pointer);
+			m_targets.erase(found);
+		}
+		Buffer b;
+		b.bytes = needed;
+		if (cudaMalloc(&b.pointer, needed) != cudaSuccess)
+		{
+			return RESTIR_ERROR_OUT_OF_MEMORY;
+		}
+		m_targets["gi.workspace"] = b;
+		return RESTIR_OK;
+	}
+
 	bool targetsMatch(const RestirParams& P) const
 	{
 		return !m_targets.empty() && P.width == m_width && P.height == m_height && P.gi_width == m_giWidth
@@ -512,6 +544,12 @@ private:
 			plan.denoiser ? p<uint16_t>("filtered" + R) : p<uint16_t>("gi.color" + R), p<uint16_t>("gi.moments" + R) };
 		RestirGiReservoirs current = { p<float>("gi.sample" + H), p<float>("gi.receiver" + H), p<float>("gi.normal" + H) };
 		run(RESTIR_PASS_GI_TEMPORAL, [&] {
+			if (m_settings.wavefront)
+			{
+				const Buffer& w = m_targets["gi.workspace"];
+				return restir_gi_temporal_wavefront(&P, &scene, &gb, &history, p<uint32_t>("grid" + R), p<float>("shadow.atlas"),
+					surface, &current, w.pointer, w.bytes, s);
+			}
 			return restir_gi_temporal(&P, &scene, &gb, &history, p<uint32_t>("grid" + R), p<float>("shadow.atlas"), surface,
 				&current, s);
 		});

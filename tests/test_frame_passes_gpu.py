@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import restir_b200 as rb
-from oracle.frame import run_checked
+from oracle.frame import FrameRunner, run_checked
 from tests.helpers import make_scene
 
 CASES = {
@@ -27,9 +27,7 @@ CASES = {
 }
 
 
-@pytest.mark.gpu
-@pytest.mark.parametrize("case", list(CASES))
-def test_frame_passes_bit_exact(case):
+def _case_setup(case):
     c = CASES[case]
     kind, seed, tris = c["scene"]
     setup = make_scene(kind, seed, tris, extra_lights=c["overrides"].get("extra_lights", 0))
@@ -39,6 +37,13 @@ def test_frame_passes_bit_exact(case):
     settings.grid_mode = rb.GRID_DETERMINISTIC
     if "extra_lights" in c["overrides"]:
         setup.lights = rb.Lights(setup.bvh, setup.mesh, settings)
+    return c, setup, settings
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", list(CASES))
+def test_frame_passes_bit_exact(case):
+    c, setup, settings = _case_setup(case)
     w, h = c["size"]
     report, oracle_run, cuda_run = run_checked(setup, w, h, c["frames"], settings)
     assert report == {}, report
@@ -47,6 +52,43 @@ def test_frame_passes_bit_exact(case):
     assert np.count_nonzero(hdr[:, :3]) > 0.2 * hdr[:, :3].size
     gi = oracle_run.host("gi.color1" if oracle_run.history_read == 1 else "gi.color0")
     assert np.count_nonzero(gi) > 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", list(CASES))
+def test_gi_temporal_wavefront_bit_exact(case):
+    """The wavefront GI temporal pass (candidates, queued tracer, shading)
+    reproduces the oracle's reservoirs bit for bit, like the single-kernel pass."""
+    c, setup, settings = _case_setup(case)
+    w, h = c["size"]
+    rb.status_flags()
+    report, _, cuda_run = run_checked(setup, w, h, c["frames"], settings, gi_wavefront=True)
+    assert report == {}, report
+    assert cuda_run.gi_workspace is not None
+    assert rb.status_flags() & 4 == 0  # no queue overflow
+
+
+@pytest.mark.gpu
+def test_gi_temporal_wavefront_rejects_bad_workspace():
+    import torch
+    setup = make_scene(rb.SCENE_CORNELL)
+    runner = FrameRunner(setup, 32, 32, "cuda", gi_wavefront=True)
+    P, _ = runner.prepare()
+    lib = runner.lib
+    nbytes = int(lib.restir_gi_temporal_workspace_bytes(P))
+    n = P.gi_width * P.gi_height * P.initial_candidates
+    assert nbytes == 256 + sum((b * n + 255) // 256 * 256 for b in (32, 4, 4, 16, 4))
+    space = torch.zeros(nbytes + 256, dtype=torch.uint8, device="cuda")
+    from restir_b200.abi import RestirGiHistory, RestirGiReservoirs
+    hist = RestirGiHistory(runner.b("gi.sample0"), runner.b("gi.receiver0"), runner.b("gi.normal0"),
+                           runner.b("gi.color0"), runner.b("gi.moments0"))
+    cur = RestirGiReservoirs(runner.b("gi.sample1"), runner.b("gi.receiver1"), runner.b("gi.normal1"))
+    args = (P, runner.scene, runner.gbuffer(), hist, runner.b("grid0"), runner.b("atlas"), runner.b("gb.emissive"), cur)
+    # Misaligned, too small, missing.
+    assert lib.restir_gi_temporal_wavefront(*args, space.data_ptr() + 16, nbytes, None) == rb.ERROR_INVALID_ARGUMENT
+    assert lib.restir_gi_temporal_wavefront(*args, space.data_ptr(), nbytes - 1, None) == rb.ERROR_INVALID_ARGUMENT
+    assert lib.restir_gi_temporal_wavefront(*args, None, nbytes, None) == rb.ERROR_INVALID_ARGUMENT
+    torch.cuda.synchronize()
 
 
 @pytest.mark.gpu

@@ -11,7 +11,8 @@ import restir_b200 as rb
 from tests.helpers import make_scene, seeded_rays
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
-KINDS = [rb.TRACE_CLOSEST, rb.TRACE_ANY, rb.TRACE_CLOSEST_STACKLESS, rb.TRACE_CLOSEST_WATERTIGHT]
+KINDS = [rb.TRACE_CLOSEST, rb.TRACE_ANY, rb.TRACE_CLOSEST_STACKLESS, rb.TRACE_CLOSEST_WATERTIGHT,
+         rb.TRACE_CLOSEST_QUEUE]
 
 
 def trace_both(setup, rays, kind, scene_host=None, scene_dev=None):
