@@ -317,7 +317,9 @@ int restir_error_noalloc(const RestirParams* params, const uint16_t* display, co
 
 /* Reads and clears the device status word: bit 0 a traversal reached its
  * step cap, bit 1 a hash grid probe sequence was exhausted, bit 2 a ray
- * queue was full (rays past its capacity are not traced). */
+ * queue was full (rays past its capacity are not traced), bit 3 a
+ * tensor-core step of the radiance cache failed (a bounded wait gave up or a
+ * shared-memory tile was misaligned; that launch's results are invalid). */
 int restir_status(uint32_t* flags);
 
 /* Work counters: waits for the device, returns the counts gathered since the

@@ -273,6 +273,25 @@ RN_HD float rn_unorm8_to_float(uint8_t u)
 	return (float)u / 255.0f;
 }
 
+/* bfloat16 (the upper half of binary32) from binary32, rounded to nearest
+ * even; NaN stays a quiet NaN. Used by the radiance cache's network inputs,
+ * weights and activations. */
+RN_HD uint16_t rn_float_to_bf16(float f)
+{
+	uint32_t x = rn_float_bits(f);
+	if ((x & 0x7fffffffu) > 0x7f800000u)
+	{
+		return (uint16_t)((x >> 16) | 0x40u);
+	}
+	uint32_t rounding = 0x7fffu + ((x >> 16) & 1u);
+	return (uint16_t)((x + rounding) >> 16);
+}
+
+RN_HD float rn_bf16_to_float(uint16_t b)
+{
+	return rn_bits_float((uint32_t)b << 16);
+}
+
 #ifdef __cplusplus
 }
 #endif

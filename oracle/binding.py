@@ -46,6 +46,11 @@ _SIGNATURES = {
     "oracle_grid_keys": (None, [P, P, u32, P, P, P, u32, P, P, P]),
     "oracle_set_threads": (None, [C.c_int]),
     "oracle_get_threads": (C.c_int, []),
+    # radiance cache (oracle_cache.cpp): config and layout pointers first
+    "oracle_cache_features": (None, [P, P, P, P, u32, P]),
+    "oracle_cache_forward": (None, [P, P, u32, P]),
+    "oracle_cache_gradients": (None, [P, P, P, P, P, P, u32, C.c_float, P, P, P]),
+    "oracle_cache_adam": (None, [P, u32, P, P, P, P, C.c_float, C.c_float]),
 }
 
 _lib = None

@@ -108,6 +108,17 @@ _SIGNATURES = {
     "restir_renderer_last_frame": (C.c_int, [P, C.POINTER(RestirParams), C.POINTER(RestirFramePlan),
                                              C.POINTER(RestirFrameState)]),
     "restir_renderer_buffer": (C.c_int, [P, C.c_char_p, C.POINTER(P), C.POINTER(C.c_uint64)]),
+    # restir_cache.h
+    "restir_cache_config_default": (None, [C.POINTER(abi.RestirCacheConfig)]),
+    "restir_cache_layout": (C.c_int, [C.POINTER(abi.RestirCacheConfig), C.POINTER(abi.RestirCacheLayout)]),
+    "restir_cache_state_bytes": (C.c_uint64, [C.POINTER(abi.RestirCacheConfig)]),
+    "restir_cache_init": (C.c_int, [C.POINTER(abi.RestirCacheConfig), P, P]),
+    "restir_cache_query": (C.c_int, [C.POINTER(abi.RestirCacheConfig), P, P, u32, P, P]),
+    "restir_cache_features": (C.c_int, [C.POINTER(abi.RestirCacheConfig), P, P, u32, P, P]),
+    "restir_cache_forward": (C.c_int, [C.POINTER(abi.RestirCacheConfig), P, P, u32, P, P]),
+    "restir_cache_gradients": (C.c_int, [C.POINTER(abi.RestirCacheConfig), P, P, P, u32, P]),
+    "restir_cache_adam": (C.c_int, [C.POINTER(abi.RestirCacheConfig), P, P]),
+    "restir_cache_train": (C.c_int, [C.POINTER(abi.RestirCacheConfig), P, P, P, u32, P]),
 }
 
 
@@ -383,3 +394,85 @@ def status_flags() -> int:
     flags = C.c_uint32(0)
     check(load().restir_status(C.byref(flags)), "restir_status")
     return flags.value
+
+
+def cache_config(**overrides) -> abi.RestirCacheConfig:
+    """restir_cache_config_default with the given fields replaced."""
+    cfg = abi.RestirCacheConfig()
+    load().restir_cache_config_default(C.byref(cfg))
+    for key, value in overrides.items():
+        if key in ("bounds_min", "bounds_max"):
+            getattr(cfg, key)[:] = list(value)
+        else:
+            setattr(cfg, key, value)
+    return cfg
+
+
+def cache_layout(cfg: abi.RestirCacheConfig) -> abi.RestirCacheLayout:
+    layout = abi.RestirCacheLayout()
+    check(load().restir_cache_layout(C.byref(cfg), C.byref(layout)), "restir_cache_layout")
+    return layout
+
+
+class RadianceCache:
+    """The radiance cache of include/restir_cache.h with its state in one torch
+    device buffer; queries and targets are torch float32 tensors on the GPU
+    ((n, 16) and (n, 4))."""
+
+    def __init__(self, cfg: abi.RestirCacheConfig | None = None, stream: int | None = None):
+        import torch
+        self.cfg = cfg or cache_config()
+        self.layout = cache_layout(self.cfg)
+        self._lib = load()
+        self.state = torch.zeros(self.layout.bytes, dtype=torch.uint8, device="cuda")
+        assert self.state.data_ptr() % 256 == 0
+        self.stream = stream
+        check(self._lib.restir_cache_init(C.byref(self.cfg), self.state.data_ptr(), stream), "restir_cache_init")
+
+    def region(self, name: str, dtype, count: int | None = None):
+        """A view of one region of the state (see RestirCacheLayout)."""
+        import torch
+        offset = getattr(self.layout, name)
+        itemsize = torch.empty((), dtype=dtype).element_size()
+        if count is None:
+            ends = sorted(getattr(self.layout, f) for f, _ in abi.RestirCacheLayout._fields_[:13])
+            count = (ends[ends.index(offset) + 1] - offset) // itemsize
+        return self.state[offset:offset + count * itemsize].view(dtype)
+
+    def query(self, queries, out=None):
+        import torch
+        n = queries.shape[0]
+        out = out if out is not None else torch.empty((n, 4), dtype=torch.float16, device="cuda")
+        check(self._lib.restir_cache_query(C.byref(self.cfg), self.state.data_ptr(), queries.data_ptr(), n,
+                                           out.data_ptr(), self.stream), "restir_cache_query")
+        return out
+
+    def forward(self, queries):
+        import torch
+        out = torch.empty((queries.shape[0], 16), dtype=torch.float32, device="cuda")
+        check(self._lib.restir_cache_forward(C.byref(self.cfg), self.state.data_ptr(), queries.data_ptr(),
+                                             queries.shape[0], out.data_ptr(), self.stream), "restir_cache_forward")
+        return out
+
+    def features(self, queries):
+        import torch
+        out = torch.empty((queries.shape[0], 64), dtype=torch.int16, device="cuda")
+        check(self._lib.restir_cache_features(C.byref(self.cfg), self.state.data_ptr(), queries.data_ptr(),
+                                              queries.shape[0], out.data_ptr(), self.stream), "restir_cache_features")
+        return out
+
+    def gradients(self, queries, targets) -> None:
+        check(self._lib.restir_cache_gradients(C.byref(self.cfg), self.state.data_ptr(), queries.data_ptr(),
+                                               targets.data_ptr(), queries.shape[0], self.stream),
+              "restir_cache_gradients")
+
+    def adam(self) -> None:
+        check(self._lib.restir_cache_adam(C.byref(self.cfg), self.state.data_ptr(), self.stream), "restir_cache_adam")
+
+    def train(self, queries, targets) -> None:
+        check(self._lib.restir_cache_train(C.byref(self.cfg), self.state.data_ptr(), queries.data_ptr(),
+                                           targets.data_ptr(), queries.shape[0], self.stream), "restir_cache_train")
+
+    def scalars(self) -> abi.RestirCacheScalars:
+        raw = self.state[self.layout.scalars:self.layout.scalars + C.sizeof(abi.RestirCacheScalars)].cpu().numpy()
+        return abi.RestirCacheScalars.from_buffer_copy(raw.tobytes())

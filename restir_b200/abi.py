@@ -130,3 +130,37 @@ class RestirFramePlan(C.Structure):
         ("reference_accumulate", C.c_int), ("reference_weight_frames", C.c_uint32),
         ("surface_light_is_di", C.c_int),
     ]
+
+
+# --- include/restir_cache.h ---------------------------------------------------------------------------
+
+CACHE_LEVELS = 16
+CACHE_FEATURES = 2
+CACHE_WEIGHTS = 4 * 64 * 64 + 16 * 64
+CACHE_PARTIAL_STRIDE = CACHE_WEIGHTS + 64
+
+
+class RestirCacheConfig(C.Structure):
+    _fields_ = [
+        ("bounds_min", f3), ("bounds_max", f3), ("table_log2", C.c_uint32), ("n_min", C.c_float),
+        ("n_max", C.c_float), ("learning_rate", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float),
+        ("epsilon", C.c_float), ("initial_loss_scale", C.c_float), ("seed", C.c_uint32),
+    ]
+
+
+class RestirCacheLayout(C.Structure):
+    _fields_ = [
+        ("weights", C.c_uint64), ("weights_bf16", C.c_uint64), ("weight_m", C.c_uint64), ("weight_v", C.c_uint64),
+        ("weight_grad", C.c_uint64), ("weight_partials", C.c_uint64), ("table", C.c_uint64),
+        ("table_half", C.c_uint64), ("table_m", C.c_uint64), ("table_v", C.c_uint64), ("table_grad", C.c_uint64),
+        ("scalars", C.c_uint64), ("bytes", C.c_uint64), ("entries", C.c_uint32), ("partial_blocks", C.c_uint32),
+        ("level_scale", C.c_float * CACHE_LEVELS), ("level_dense", C.c_uint32 * CACHE_LEVELS),
+    ]
+
+
+class RestirCacheScalars(C.Structure):
+    _fields_ = [
+        ("loss_scale", C.c_float), ("step", C.c_uint32), ("clean_steps", C.c_uint32), ("skipped_steps", C.c_uint32),
+        ("loss", C.c_float), ("nonfinite", C.c_uint32), ("samples", C.c_uint32), ("blocks", C.c_uint32),
+        ("beta1_power", C.c_float), ("beta2_power", C.c_float), ("pad", C.c_uint32 * 6),
+    ]
