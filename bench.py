@@ -60,6 +60,9 @@ PASS_PIXEL_BYTES = {
     "denoise": ("gi", 56 + 5 * 48),
     "composite": ("full", 50),
     "reference": ("full", 57),
+    # radiance-cache training: per training sample a query and a target (80 B) and the hash-grid
+    # gather of two queries (2 x 512 B); counted per GI pixel only when it runs
+    "cache": ("none", 0),
 }
 
 

@@ -34,13 +34,18 @@
  *
  * Memory: one caller-owned device block of restir_cache_state_bytes, 256-byte
  * aligned; restir_cache_layout gives the byte offset of every region in it.
- * Queries: 16 floats each, (position xyz, roughness), (normal xyz, 0),
- * (direction xyz, 0), (albedo rgb, 0). Targets: 4 floats, (rgb, 0).
+ * Queries: 16 floats each, (position xyz, roughness), (normal xyz, valid),
+ * (direction xyz, 0), (albedo rgb, 0); valid is 1 for a query and 0 for a
+ * padding row, whose value comes back with alpha 0. Targets: 4 floats,
+ * (rgb, weight); a sample's loss and gradient are scaled by its weight (0
+ * drops it).
  */
 #ifndef RESTIR_CACHE_H
 #define RESTIR_CACHE_H
 
 #include <stdint.h>
+
+#include "restir_gpu.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -126,8 +131,8 @@ uint64_t restir_cache_state_bytes(const RestirCacheConfig* cfg);
  * features uniform in +-1e-4, moments and gradients zero. */
 int restir_cache_init(const RestirCacheConfig* cfg, void* state, void* stream);
 
-/* The cache's value (max(output, 0) in rgb, 1 in alpha) for n queries, as
- * half4. */
+/* The cache's value (max(output, 0) in rgb, the query's valid flag in
+ * alpha) for n queries, as half4. */
 int restir_cache_query(const RestirCacheConfig* cfg, const void* state, const float* queries, uint32_t n,
 	uint16_t* output, void* stream);
 
@@ -152,6 +157,41 @@ int restir_cache_adam(const RestirCacheConfig* cfg, void* state, void* stream);
 /* restir_cache_gradients then restir_cache_adam. */
 int restir_cache_train(const RestirCacheConfig* cfg, void* state, const float* queries, const float* targets,
 	uint32_t n, void* stream);
+
+/* --- the cache in the GI passes (params->radiance_cache > 0.5) ---------- */
+
+/* restir_gi_temporal_wavefront with the cache standing in for
+ * previousIndirect at every sample point the pass shades: the candidates'
+ * hits and last frame's reservoirs' samples each get a query row (the
+ * point's surface as evaluateSample finds it, the direction toward its
+ * receiver), answered in one restir_cache_query before the shading.
+ * workspace: restir_gi_temporal_workspace_bytes(params) (which includes the
+ * cache's rows and the training batch when params->radiance_cache is set).
+ * The rows: candidate (pixel * initial_candidates + k) first, then last
+ * frame's reservoir i at GI pixels x initial_candidates + i; the values
+ * (half4) follow the same order. */
+int restir_gi_temporal_cached(const RestirParams* params, const RestirScene* scene, const RestirGBuffer* gbuffer,
+	const RestirGiHistory* history, const uint32_t* previous_grid, const float* shadow_atlas,
+	const uint16_t* surface_light, const RestirGiReservoirs* output, const RestirCacheConfig* cache_config,
+	const void* cache_state, void* workspace, uint64_t workspace_bytes, void* stream);
+
+/* restir_gi_spatial with the cache's values for this frame's reservoirs
+ * (rows 0 .. GI pixels - 1 of the same workspace). */
+int restir_gi_spatial_cached(const RestirParams* params, const RestirScene* scene, const RestirGBuffer* gbuffer,
+	const RestirGiReservoirs* current, const uint32_t* current_grid, const RestirGiHistory* history,
+	const float* shadow_atlas, const uint16_t* surface_light, uint16_t* color, uint16_t* moments,
+	const RestirCacheConfig* cache_config, const void* cache_state, void* workspace, uint64_t workspace_bytes,
+	void* stream);
+
+/* One training step on params->cache_training_samples path suffixes: each
+ * starts at a seeded GI pixel's G-buffer surface, takes a cosine-distributed
+ * direction and its first hit through the BVH; the target is the light
+ * leaving that hit toward the start (point light with the shadow atlas, the
+ * triangle's emission, the sky on a miss) plus the hit's albedo times the
+ * cache's own value there. */
+int restir_cache_train_frame(const RestirParams* params, const RestirScene* scene, const RestirGBuffer* gbuffer,
+	const float* shadow_atlas, const RestirCacheConfig* cache_config, void* cache_state, void* workspace,
+	uint64_t workspace_bytes, void* stream);
 
 #ifdef __cplusplus
 }

@@ -63,6 +63,10 @@ typedef struct RestirSettings
 	uint32_t grid_mode;      /* RESTIR_GRID_* */
 	uint32_t wavefront;      /* no reference counterpart: 1 runs the GI temporal pass as
 	                            restir_gi_temporal_wavefront (same output), 0 as restir_gi_temporal */
+	uint32_t radiance_cache; /* no reference counterpart: 1 takes the indirect light at GI
+	                            sample points from the radiance cache (restir_cache.h),
+	                            trained every frame; needs wavefront */
+	uint32_t cache_training_samples;  /* path suffixes per frame (default 65,536) */
 } RestirSettings;
 
 /* FrameInput (renderer.h) with the fly camera's pose. */
@@ -123,7 +127,8 @@ void restir_frame_advance(const RestirParams* params, const RestirFramePlan* pla
 #define RESTIR_PASS_DENOISE 7
 #define RESTIR_PASS_COMPOSITE 8
 #define RESTIR_PASS_REFERENCE 9
-#define RESTIR_PASS_COUNT 10
+#define RESTIR_PASS_CACHE 10      /* radiance-cache training (no reference counterpart) */
+#define RESTIR_PASS_COUNT 11
 
 typedef struct RestirMetrics
 {

@@ -135,6 +135,13 @@ typedef struct RestirParams
 	float sky_ground[4];         /* u_skyGround */
 
 	float composite_options[4];  /* u_compositeOptions */
+	/* No reference counterpart: > 0.5 when the GI passes take the indirect
+	 * light leaving a sample point from the radiance cache
+	 * (restir_gi_temporal_cached, restir_gi_spatial_cached) instead of
+	 * previousIndirect (restir.sh:265-298). */
+	float radiance_cache;
+	uint32_t cache_training_samples;  /* path suffixes traced per frame to train it */
+	float pad_params[2];
 } RestirParams;
 
 /* Scene buffers, uploaded once per scene (renderer.cpp:365-419, 1170-1207). */

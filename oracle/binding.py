@@ -36,6 +36,10 @@ _SIGNATURES = {
     "oracle_gi_temporal": (C.c_int, [PP, PS, PG, C.POINTER(RestirGiHistory), P, P, P, C.POINTER(RestirGiReservoirs)]),
     "oracle_gi_spatial": (C.c_int, [PP, PS, PG, C.POINTER(RestirGiReservoirs), P, C.POINTER(RestirGiHistory), P, P,
                                     P, P]),
+    "oracle_gi_temporal_cached": (C.c_int, [PP, PS, PG, C.POINTER(RestirGiHistory), P, P, P,
+                                            C.POINTER(RestirGiReservoirs), P]),
+    "oracle_gi_spatial_cached": (C.c_int, [PP, PS, PG, C.POINTER(RestirGiReservoirs), P, C.POINTER(RestirGiHistory),
+                                           P, P, P, P, P]),
     "oracle_svgf_variance": (C.c_int, [PP, P, P, P, P, P]),
     "oracle_svgf_atrous": (C.c_int, [PP, C.c_int, P, P, P, P]),
     "oracle_composite": (C.c_int, [PP, PG, P, P, P, P, P]),

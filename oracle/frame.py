@@ -76,6 +76,17 @@ class FrameRunner:
             self.scene = setup.host_scene()
             self.lib = ob.load()
         self.error_scratch = None
+        # The radiance cache (settings.radiance_cache): the cuda backend owns it;
+        # the oracle backend takes its values per pass (cache_values) from there.
+        self.radiance_cache = p.radiance_cache > 0.5
+        self.cache = None
+        self.cache_values = None
+        if self.radiance_cache and backend == "cuda":
+            desc = setup.mesh.desc
+            lo = [desc.bounds_min[i] - 0.01 * desc.radius for i in range(3)]
+            hi = [desc.bounds_max[i] + 0.01 * desc.radius for i in range(3)]
+            self.cache = rb.RadianceCache(rb.cache_config(bounds_min=lo, bounds_max=hi))
+            self.gi_wavefront = True
 
     # --- pass plumbing --------------------------------------------------------------------------------
 
@@ -128,15 +139,34 @@ class FrameRunner:
         history = RestirGiHistory(self.b(f"gi.sample{hr}"), self.b(f"gi.receiver{hr}"), self.b(f"gi.normal{hr}"),
                                   color_read, self.b(f"gi.moments{hr}"))
         current = RestirGiReservoirs(self.b(f"gi.sample{hw}"), self.b(f"gi.receiver{hw}"), self.b(f"gi.normal{hw}"))
-        if self.gi_wavefront:
-            out.append(("gi_temporal", lambda: self.gi_temporal_wavefront(P, gb, history, self.b(f"grid{hr}"), surface,
-                                                                          current)))
+        if self.radiance_cache and self.backend == "cuda":
+            out.append(("gi_temporal", lambda: self.cached_pass(
+                "gi_temporal_cached", P, self.scene, gb, history, self.b(f"grid{hr}"), self.b("atlas"), surface,
+                current)))
+            out.append(("gi_spatial", lambda: self.cached_pass(
+                "gi_spatial_cached", P, self.scene, gb, current, self.b(f"grid{hw}"), history, self.b("atlas"),
+                surface, self.b(f"gi.color{hw}"), self.b(f"gi.moments{hw}"))))
+            out.append(("cache_train", lambda: self.cached_pass("cache_train_frame", P, self.scene, gb,
+                                                                self.b("atlas"))))
+        elif self.radiance_cache:
+            out.append(("gi_temporal", lambda: self.call(
+                "gi_temporal_cached", P, self.scene, gb, history, self.b(f"grid{hr}"), self.b("atlas"), surface,
+                current, self.cache_values.ctypes.data)))
+            out.append(("gi_spatial", lambda: self.call(
+                "gi_spatial_cached", P, self.scene, gb, current, self.b(f"grid{hw}"), history, self.b("atlas"),
+                surface, self.b(f"gi.color{hw}"), self.b(f"gi.moments{hw}"), self.cache_values.ctypes.data)))
+            out.append(("cache_train", lambda: None))
         else:
-            out.append(("gi_temporal", lambda: self.call("gi_temporal", P, self.scene, gb, history,
-                                                         self.b(f"grid{hr}"), self.b("atlas"), surface, current)))
-        out.append(("gi_spatial", lambda: self.call("gi_spatial", P, self.scene, gb, current, self.b(f"grid{hw}"),
-                                                    history, self.b("atlas"), surface, self.b(f"gi.color{hw}"),
-                                                    self.b(f"gi.moments{hw}"))))
+            if self.gi_wavefront:
+                out.append(("gi_temporal", lambda: self.gi_temporal_wavefront(P, gb, history, self.b(f"grid{hr}"),
+                                                                              surface, current)))
+            else:
+                out.append(("gi_temporal", lambda: self.call("gi_temporal", P, self.scene, gb, history,
+                                                             self.b(f"grid{hr}"), self.b("atlas"), surface,
+                                                             current)))
+            out.append(("gi_spatial", lambda: self.call("gi_spatial", P, self.scene, gb, current,
+                                                        self.b(f"grid{hw}"), history, self.b("atlas"), surface,
+                                                        self.b(f"gi.color{hw}"), self.b(f"gi.moments{hw}"))))
         denoised = f"gi.color{hw}"
         if plan.denoiser:
             out.append(("svgf_variance", lambda: self.call("svgf_variance", P, self.b(f"gi.color{hw}"),
@@ -168,6 +198,32 @@ class FrameRunner:
         rb.check(self.lib.restir_gi_temporal_wavefront(P, self.scene, gb, history, grid, self.b("atlas"), surface,
                                                         current, self.gi_workspace.data_ptr(), nbytes, None),
                  "gi_temporal_wavefront")
+
+    def workspace(self, P):
+        import torch
+        nbytes = int(self.lib.restir_gi_temporal_workspace_bytes(P))
+        if self.gi_workspace is None or self.gi_workspace.numel() < nbytes:
+            self.gi_workspace = torch.zeros(nbytes, dtype=torch.uint8, device="cuda")
+        assert self.gi_workspace.data_ptr() % 256 == 0
+        return self.gi_workspace.data_ptr(), nbytes
+
+    def cached_pass(self, name, *args):
+        """A cuda pass of the radiance-cache path: its arguments, then the cache
+        config and state and the GI workspace."""
+        import ctypes as C
+        pointer, nbytes = self.workspace(args[0])
+        rb.check(getattr(self.lib, "restir_" + name)(*args, C.byref(self.cache.cfg), self.cache.state.data_ptr(), pointer,
+                                                     nbytes, None), name)
+
+    def cache_value_rows(self, P):
+        """Host copy of the cache values the last cached pass read (half4 rows,
+        candidates then reservoirs), from the workspace layout of
+        restir_gi_temporal_workspace_bytes."""
+        n = P.gi_width * P.gi_height * max(P.initial_candidates, 0)
+        rows = n + P.gi_width * P.gi_height
+        up = lambda b: (b + 255) // 256 * 256
+        offset = up(8) + up(32 * n) + up(4 * n) + up(4 * n) + up(16 * n) + up(4 * n) + up(64 * rows)
+        return self.gi_workspace[offset:offset + 8 * rows].cpu().numpy().view(np.uint16).copy()
 
     def finish(self):
         rb.advance(self.params, self.plan, self.frame_input, self.state)
@@ -223,6 +279,7 @@ def run_checked(setup, width: int, height: int, frames: int, settings=None, on_m
     import torch
     oracle_run = FrameRunner(setup, width, height, "oracle", settings)
     cuda_run = FrameRunner(setup, width, height, "cuda", settings, gi_wavefront=gi_wavefront)
+    assert oracle_run.radiance_cache == cuda_run.radiance_cache
     report = {}
     for frame in range(frames):
         if reference_frames and frame == frames - reference_frames:
@@ -232,13 +289,22 @@ def run_checked(setup, width: int, height: int, frames: int, settings=None, on_m
         cuda_run.prepare()
         for (name, o_fn), (_, c_fn) in zip(oracle_run.passes(), cuda_run.passes()):
             before = {k: v.copy() for k, v in oracle_run.buffers.items()}
-            o_fn()
-            changed = [k for k in before if not np.array_equal(before[k], oracle_run.buffers[k])]
             # The CUDA pass gets exactly the oracle's inputs.
             for k, v in before.items():
                 cuda_run.buffers[k].copy_(torch.from_numpy(v))
-            c_fn()
-            torch.cuda.synchronize()
+            if cuda_run.radiance_cache and name in ("gi_temporal", "gi_spatial", "cache_train"):
+                # The cache lives on the GPU: the CUDA pass runs first and the
+                # oracle takes the cache values it read.
+                c_fn()
+                torch.cuda.synchronize()
+                if name != "cache_train":
+                    oracle_run.cache_values = cuda_run.cache_value_rows(cuda_run.params)
+                o_fn()
+            else:
+                o_fn()
+                c_fn()
+                torch.cuda.synchronize()
+            changed = [k for k in before if not np.array_equal(before[k], oracle_run.buffers[k])]
             for k in changed + [k for k in before if k not in changed and name.startswith("grid")]:
                 got = cuda_run.host(k)
                 want = oracle_run.buffers[k]

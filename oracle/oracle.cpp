@@ -356,15 +356,21 @@ struct TemporalThread
 
 } // namespace
 
-extern "C" int oracle_gi_temporal(const RestirParams* P, const RestirScene* scene, const RestirGBuffer* gb,
+/* cache_values (half4 per slot, null for the plain pass): the radiance
+ * cache's values for the candidates (slot pixel * initial_candidates + k)
+ * then last frame's reservoirs (slot GI pixels * initial_candidates + pixel),
+ * standing in for previousIndirect as in restir_gi_temporal_cached. */
+extern "C" int oracle_gi_temporal_cached(const RestirParams* P, const RestirScene* scene, const RestirGBuffer* gb,
 	const RestirGiHistory* history, const uint32_t* previous_grid, const float* shadow_atlas,
-	const uint16_t* surface_light, const RestirGiReservoirs* out)
+	const uint16_t* surface_light, const RestirGiReservoirs* out, const uint16_t* cache_values)
 {
 	resetCounts();
 	GiPass base = makeGiPass(P, scene, gb, history, shadow_atlas, surface_light);
 	base.sharedStack = true;
 	base.grid = makeGrid(P, previous_grid, P->prev_camera_position);
 	const int w = int(P->gi_width), h = int(P->gi_height);
+	base.cache = cache_values;
+	base.cacheNeighbourBase = w * h * P->initial_candidates;
 	TexF4 historySample = { history->sample, w, h };
 	const int groupsX = (w + 3) / 4, groupsY = (h + 7) / 8;
 const int threadCount = threads();
@@ -434,7 +440,9 @@ const int threadCount = threads();
 					bool evaluated = false;
 					if (hit)
 					{
-						evaluated = g.evaluateSample(t.position, t.normal, t.albedo, hitPosition, hitId, contribution, hitNormal);
+						const int cacheSlot = g.cache != nullptr ? (py * w + px) * P->initial_candidates + sampleIndex : -1;
+						evaluated = g.evaluateSample(t.position, t.normal, t.albedo, hitPosition, hitId, contribution, hitNormal,
+							cacheSlot);
 					}
 					if (evaluated)
 					{
@@ -504,6 +512,7 @@ const int threadCount = threads();
 							GiPass::skipNeighbour(t.mis);
 							continue;
 						}
+						neighbour.cacheSlot = g.cache != nullptr ? g.cacheNeighbourBase + texelIndex(historyUv, w, h) : -1;
 						g.addNeighbour(t.mis, t.position, t.normal, t.albedo, neighbour, randomSelect);
 					}
 					t.combinedWeight = g.finishPairwiseMis(t.mis, t.position, t.normal, canonical, t.canonicalWeight, nextRandom(rng));
@@ -566,17 +575,29 @@ const int threadCount = threads();
 	return RESTIR_OK;
 }
 
+extern "C" int oracle_gi_temporal(const RestirParams* P, const RestirScene* scene, const RestirGBuffer* gb,
+	const RestirGiHistory* history, const uint32_t* previous_grid, const float* shadow_atlas,
+	const uint16_t* surface_light, const RestirGiReservoirs* out)
+{
+	return oracle_gi_temporal_cached(P, scene, gb, history, previous_grid, shadow_atlas, surface_light, out, nullptr);
+}
+
 /* --- ReSTIR GI spatial (cs_restir_spatial.sc) ---------------------------- */
 
-extern "C" int oracle_gi_spatial(const RestirParams* P, const RestirScene* scene, const RestirGBuffer* gb,
+/* cache_values: the radiance cache's values for this frame's reservoirs
+ * (slot = pixel), as in restir_gi_spatial_cached; null for the plain pass. */
+extern "C" int oracle_gi_spatial_cached(const RestirParams* P, const RestirScene* scene, const RestirGBuffer* gb,
 	const RestirGiReservoirs* current, const uint32_t* current_grid, const RestirGiHistory* history,
-	const float* shadow_atlas, const uint16_t* surface_light, uint16_t* color_out, uint16_t* moments_out)
+	const float* shadow_atlas, const uint16_t* surface_light, uint16_t* color_out, uint16_t* moments_out,
+	const uint16_t* cache_values)
 {
 	resetCounts();
 	GiPass base = makeGiPass(P, scene, gb, history, shadow_atlas, surface_light);
 	base.sharedStack = false;
 	base.grid = makeGrid(P, current_grid, P->camera_position);
 	const int w = int(P->gi_width), h = int(P->gi_height);
+	base.cache = cache_values;
+	base.cacheNeighbourBase = 0;
 	TexF4 reservoirSample = { current->sample, w, h };
 	TexF4 reservoirReceiver = { current->receiver, w, h };
 	TexF4 reservoirNormal = { current->normal, w, h };
@@ -618,7 +639,8 @@ const int threadCount = threads();
 				if (canonicalWeight > 0.0f)
 				{
 					canonicalValid = g.evaluateSample(position, normal, albedo, ownSample.xyz(),
-						reservoirNormal.sample(v_texcoord0).w, canonicalContribution, canonicalNormal);
+						reservoirNormal.sample(v_texcoord0).w, canonicalContribution, canonicalNormal,
+						g.cache != nullptr ? texelIndex(v_texcoord0, w, h) : -1);
 				}
 				if (canonicalValid)
 				{
@@ -664,6 +686,7 @@ const int threadCount = threads();
 						GiPass::skipNeighbour(mis);
 						continue;
 					}
+					neighbour.cacheSlot = g.cache != nullptr ? texelIndex(neighbourUv, w, h) : -1;
 					g.addNeighbour(mis, position, normal, albedo, neighbour, randomSelect);
 				}
 
@@ -735,6 +758,14 @@ const int threadCount = threads();
 		addCounts(gs_[size_t(t_)].bvh, 0, pixelss_[size_t(t_)]);
 	}
 	return RESTIR_OK;
+}
+
+extern "C" int oracle_gi_spatial(const RestirParams* P, const RestirScene* scene, const RestirGBuffer* gb,
+	const RestirGiReservoirs* current, const uint32_t* current_grid, const RestirGiHistory* history,
+	const float* shadow_atlas, const uint16_t* surface_light, uint16_t* color_out, uint16_t* moments_out)
+{
+	return oracle_gi_spatial_cached(P, scene, gb, current, current_grid, history, shadow_atlas, surface_light, color_out,
+		moments_out, nullptr);
 }
 
 /* --- ReSTIR DI (di.sh, cs_di_temporal.sc, cs_di_spatial.sc) -------------- */

@@ -205,14 +205,16 @@ extern "C" void oracle_cache_gradients(const RestirCacheConfig* cfg, const Resti
 		forward(weights_bf16, x, acts, out);
 		// Output gradient (16 wide, 3 used).
 		uint16_t dz[64] = {};
+		const float weight = targets[size_t(i) * 4 + 3];
 		for (int c = 0; c < 3; ++c)
 		{
 			const float y = float(out[c]);
 			const float t = targets[size_t(i) * 4 + c];
 			const float denominator = y * y + 0.01f;
 			const float difference = y - t;
-			lossSum += double(difference * difference / denominator);
-			dz[c] = rn_float_to_bf16(difference / denominator * gradientScale * loss_scale);
+			const float term = difference * difference / denominator;
+			lossSum += double(weight * term);
+			dz[c] = rn_float_to_bf16(difference / denominator * gradientScale * loss_scale * weight);
 		}
 		for (int layer = 4; layer >= 0; --layer)
 		{

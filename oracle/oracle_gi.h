@@ -219,6 +219,7 @@ struct NeighbourReservoir
 	vec3 receiverNormal;
 	float count = 0.0f;
 	float weight = 0.0f;
+	int cacheSlot = -1;  // the radiance cache's value for this sample, or -1
 };
 
 struct PairwiseMis
@@ -251,6 +252,11 @@ struct GiPass
 	TexH4 historyColor, surfaceLight;
 	TexF4 historyNormal, historyReceiver;
 	vec2 giSize, giTexel;
+	// The radiance cache's values (half4 per slot), when the pass takes the
+	// indirect light at sample points from it (restir_cache.h): an input here,
+	// like a texture. Reused neighbours sit at cacheNeighbourBase + pixel.
+	const uint16_t* cache = nullptr;
+	int cacheNeighbourBase = 0;
 
 	float s() const { return P->scene_scale; }
 	float kRayBias() const { return 0.02f * s(); }
@@ -483,8 +489,24 @@ struct GiPass
 		return false;
 	}
 
+	// previousIndirect, or the radiance cache's value for the slot times the
+	// albedo (zero for a padding row).
+	vec3 sampleIndirect(vec3 _position, vec3 _normal, vec3 _albedo, int _cacheSlot) const
+	{
+		if (cache != nullptr && _cacheSlot >= 0)
+		{
+			const uint16_t* c = cache + size_t(_cacheSlot) * 4;
+			if (rn_half_to_float(c[3]) > 0.5f)
+			{
+				return vec3(rn_half_to_float(c[0]), rn_half_to_float(c[1]), rn_half_to_float(c[2])) * _albedo;
+			}
+			return vec3_splat(0.0f);
+		}
+		return previousIndirect(_position, _normal, _albedo);
+	}
+
 	bool evaluateSample(vec3 _receiverPosition, vec3 _receiverNormal, vec3 _receiverAlbedo, vec3 _samplePosition,
-		float _sampleId, vec3& _contribution, vec3& _sampleNormal) const
+		float _sampleId, vec3& _contribution, vec3& _sampleNormal, int _cacheSlot = -1) const
 	{
 		_contribution = vec3_splat(0.0f);
 		_sampleNormal = vec3(0.0f, 0.0f, 1.0f);
@@ -536,13 +558,13 @@ struct GiPass
 		if (visibleSurface)
 		{
 			radiance = evaluateSecondaryDirect(sampleUv, _samplePosition, _sampleNormal)
-				+ previousIndirect(_samplePosition, _sampleNormal, diffuseAlbedo(sampleUv))
+				+ sampleIndirect(_samplePosition, _sampleNormal, diffuseAlbedo(sampleUv), _cacheSlot)
 				+ surfaceLight.sample(sampleUv).xyz() * P->surface_light_scale;
 		}
 		else
 		{
 			radiance = evaluateWorldDirect(bvhTriangleAlbedo(bvh, triangleIndex), _samplePosition, _sampleNormal)
-				+ previousIndirect(_samplePosition, _sampleNormal, bvhTriangleAlbedo(bvh, triangleIndex))
+				+ sampleIndirect(_samplePosition, _sampleNormal, bvhTriangleAlbedo(bvh, triangleIndex), _cacheSlot)
 				+ bvhTriangleEmission(bvh, triangleIndex) * P->emission_scale;
 		}
 		_contribution = _receiverAlbedo * radiance * (receiverCosine / kPi);
@@ -700,7 +722,7 @@ struct GiPass
 		if (_neighbour.weight > 0.0f)
 		{
 			shifted = evaluateSample(_position, _normal, _albedo, _neighbour.samplePosition, _neighbour.sampleId,
-				contribution, sampleNormal);
+				contribution, sampleNormal, _neighbour.cacheSlot);
 		}
 		if (shifted)
 		{

@@ -34,7 +34,7 @@ OK, ERROR_INVALID_ARGUMENT, ERROR_LAUNCH, ERROR_STEP_CAP, ERROR_UNSUPPORTED = 0,
 ERROR_TIMEOUT, ERROR_OUT_OF_MEMORY, ERROR_TOO_LARGE = -5, -6, -7
 TRACE_CLOSEST, TRACE_ANY, TRACE_CLOSEST_STACKLESS, TRACE_CLOSEST_WATERTIGHT, TRACE_CLOSEST_QUEUE = 0, 1, 2, 3, 4
 PASS_NAMES = ["shadow", "gbuffer", "di_temporal", "di_spatial", "grid", "gi_temporal", "gi_spatial",
-              "denoise", "composite", "reference"]
+              "denoise", "composite", "reference", "cache"]
 
 _lib = None
 
@@ -119,6 +119,14 @@ _SIGNATURES = {
     "restir_cache_gradients": (C.c_int, [C.POINTER(abi.RestirCacheConfig), P, P, P, u32, P]),
     "restir_cache_adam": (C.c_int, [C.POINTER(abi.RestirCacheConfig), P, P]),
     "restir_cache_train": (C.c_int, [C.POINTER(abi.RestirCacheConfig), P, P, P, u32, P]),
+    "restir_gi_temporal_cached": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirScene), C.POINTER(RestirGBuffer),
+                                            C.POINTER(RestirGiHistory), P, P, P, C.POINTER(RestirGiReservoirs),
+                                            C.POINTER(abi.RestirCacheConfig), P, P, C.c_uint64, P]),
+    "restir_gi_spatial_cached": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirScene), C.POINTER(RestirGBuffer),
+                                           C.POINTER(RestirGiReservoirs), P, C.POINTER(RestirGiHistory), P, P, P, P,
+                                           C.POINTER(abi.RestirCacheConfig), P, P, C.c_uint64, P]),
+    "restir_cache_train_frame": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirScene), C.POINTER(RestirGBuffer),
+                                           P, C.POINTER(abi.RestirCacheConfig), P, P, C.c_uint64, P]),
 }
 
 

@@ -35,6 +35,7 @@ class RestirParams(C.Structure):
         ("shadows_enabled", C.c_float), ("shadow_face_size", C.c_uint32),
         ("sky_zenith", f4), ("sky_horizon", f4), ("sky_ground", f4),
         ("composite_options", f4),
+        ("radiance_cache", C.c_float), ("cache_training_samples", C.c_uint32), ("pad_params", C.c_float * 2),
     ]
 
 
@@ -101,7 +102,7 @@ class RestirSettings(C.Structure):
         ("initial_candidates", C.c_int), ("temporal_taps", C.c_int), ("spatial_taps", C.c_int),
         ("trace_steps", C.c_int), ("di_candidates", C.c_int), ("di_spatial_taps", C.c_int),
         ("grid_table_size", C.c_uint32), ("grid_cell_capacity", C.c_uint32), ("grid_mode", C.c_uint32),
-        ("wavefront", C.c_uint32),
+        ("wavefront", C.c_uint32), ("radiance_cache", C.c_uint32), ("cache_training_samples", C.c_uint32),
     ]
 
 
@@ -120,7 +121,7 @@ class RestirFrameState(C.Structure):
 
 class RestirMetrics(C.Structure):
     _fields_ = [("valid", C.c_int), ("relative_mse", C.c_double), ("bias", C.c_double), ("error", C.c_double * 4),
-                ("pass_ms", C.c_float * 10), ("reference_frames", C.c_uint32)]
+                ("pass_ms", C.c_float * 11), ("reference_frames", C.c_uint32)]
 
 
 class RestirFramePlan(C.Structure):

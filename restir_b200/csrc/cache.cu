@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(kTile) forwardKernel(CacheView c, const float4
 						h.x = rn_float_to_half(fmaxf(v[0], 0.0f));
 						h.y = rn_float_to_half(fmaxf(v[1], 0.0f));
 						h.z = rn_float_to_half(fmaxf(v[2], 0.0f));
-						h.w = rn_float_to_half(1.0f);
+						h.w = rn_float_to_half(queries[size_t(row) * 4 + 1].w > 0.5f ? 1.0f : 0.0f);
 						static_cast<ushort4*>(output)[row] = h;
 					}
 					else
@@ -560,13 +560,14 @@ __global__ void __launch_bounds__(kTile, 1) trainKernel(TrainArgs a)
 		{
 			const float4 target = __ldg(a.targets + row);
 			const float tv[3] = { target.x, target.y, target.z };
+			const float weight = target.w;
 			for (int ch = 0; ch < 3; ++ch)
 			{
 				const float y = prediction[ch];
 				const float denominator = y * y + 0.01f;
 				const float difference = y - tv[ch];
-				lossSum = lossSum + difference * difference / denominator;
-				g[ch] = rn_float_to_bf16(difference / denominator * gradientScale * lossScale);
+				lossSum = lossSum + weight * (difference * difference / denominator);
+				g[ch] = rn_float_to_bf16(difference / denominator * gradientScale * lossScale * weight);
 			}
 		}
 		for (int k = 0; k < 2; ++k)

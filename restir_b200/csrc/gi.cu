@@ -9,6 +9,8 @@
 #include "gi.cuh"
 #include "wavefront.cuh"
 
+#include "../../include/restir_cache.h"
+
 namespace restir
 {
 namespace
@@ -49,6 +51,8 @@ struct GiBindings
 	float4* outNormal;
 	uint16_t* outColor;              // spatial outputs
 	uint16_t* outMoments;
+	const uint16_t* cache;           // radiance-cache values (half4), or null
+	int cacheNeighbourBase;          // slot of reused neighbour 0
 };
 
 __device__ __forceinline__ GiPass makePass(const RestirParams& P, const BvhView& bvh, const GiBindings& b, const float* gridCamera,
@@ -73,6 +77,8 @@ __device__ __forceinline__ GiPass makePass(const RestirParams& P, const BvhView&
 	g.h = int(P.gi_height);
 	g.giSize = v2(float(g.w), float(g.h));
 	g.giTexel = v2(1.0f / float(g.w), 1.0f / float(g.h));
+	g.cache = b.cache;
+	g.cacheNeighbourBase = b.cacheNeighbourBase;
 	return g;
 }
 
@@ -129,6 +135,7 @@ __device__ __forceinline__ void temporalReuseAndStore(const RestirParams& P, con
 				int i = g.gi(historyUv);
 				accepted = g.acceptNeighbour(f4(__ldg(b.historySample + i)), f4(__ldg(b.historyReceiver + i)),
 					f4(__ldg(b.historyNormal + i)), position, normal, radius, neighbour);
+				neighbour.cacheSlot = g.cache != nullptr ? g.cacheNeighbourBase + i : -1;
 			}
 			if (!accepted)
 			{
@@ -316,7 +323,8 @@ __global__ void __launch_bounds__(128, RESTIR_GI_SPATIAL_MIN_BLOCKS) giSpatialKe
 	bool canonicalValid = false;
 	if (canonicalWeight > 0.0f)
 	{
-		canonicalValid = g.evaluateSample(position, normal, albedo, ownSample.xyz(), ownId, canonicalContribution, canonicalNormal);
+		canonicalValid = g.evaluateSample(position, normal, albedo, ownSample.xyz(), ownId, canonicalContribution, canonicalNormal,
+			g.cache != nullptr ? g.cacheNeighbourBase + own : -1);
 	}
 	if (canonicalValid)
 	{
@@ -363,6 +371,7 @@ __global__ void __launch_bounds__(128, RESTIR_GI_SPATIAL_MIN_BLOCKS) giSpatialKe
 			int i = g.gi(neighbourUv);
 			accepted = g.acceptNeighbour(f4(b.reservoirSample[i]), f4(b.reservoirReceiver[i]), f4(b.reservoirNormal[i]),
 				position, normal, radius, neighbour);
+			neighbour.cacheSlot = g.cache != nullptr ? g.cacheNeighbourBase + i : -1;
 		}
 		if (!accepted)
 		{
@@ -577,7 +586,8 @@ __global__ void __launch_bounds__(kGiThreads, RESTIR_GI_TEMPORAL_MIN_BLOCKS) giT
 		bool evaluated = false;
 		if (hit)
 		{
-			evaluated = g.evaluateSample(position, normal, albedo, hitPosition, hitId, contribution, hitNormal);
+			const int cacheSlot = g.cache != nullptr ? pixel * records.candidates + sampleIndex : -1;
+			evaluated = g.evaluateSample(position, normal, albedo, hitPosition, hitId, contribution, hitNormal, cacheSlot);
 		}
 		if (evaluated)
 		{
@@ -675,18 +685,41 @@ extern "C" int restir_gi_spatial(const RestirParams* params, const RestirScene* 
 	return launchStatus();
 }
 
+namespace restir
+{
 namespace
 {
+
+// The radiance cache's share of the workspace: query rows and their values
+// for the candidates then the reused reservoirs, and the training batch.
+struct CacheWorkspace
+{
+	float4* queries;        // 4 float4 per row
+	uint16_t* values;       // half4 per row
+	uint32_t rows;
+	RayQueue trainQueue;    // one suffix ray per training sample (no counter)
+	float4* trainQueries;   // at the training points
+	float4* hitQueries;     // at the suffixes' hit points
+	uint16_t* hitValues;
+	float4* partial;        // direct + emission at the hit (rgb), training weight
+	float4* hitAlbedo;
+	float4* targets;
+	uint32_t samples;
+};
 
 struct TemporalWorkspace
 {
 	RayQueue queue;
 	CandidateRecords records;
+	CacheWorkspace cache;
 	uint64_t bytes;
 };
 
 // [2 counters][rays 32 B x n][hit triangles 4 B x n][hit distances 4 B x n][screen hits 16 B x n]
-// [slots 4 B x n], each region starting on 256 bytes; n = GI pixels x initial candidates.
+// [slots 4 B x n], each region starting on 256 bytes; n = GI pixels x initial candidates. With the
+// radiance cache: [queries 64 B x r][values 8 B x r], r = n + GI pixels, then the training batch of
+// s samples: [rays 32 B][hit triangles 4 B][hit distances 4 B][2 counters][training queries 64 B]
+// [hit queries 64 B][hit values 8 B][partial 16 B][hit albedo 16 B][targets 16 B], each x s.
 TemporalWorkspace layoutTemporalWorkspace(const RestirParams* p, void* base)
 {
 	const uint64_t n = uint64_t(p->gi_width) * p->gi_height * uint64_t(p->initial_candidates > 0 ? p->initial_candidates : 0);
@@ -698,7 +731,7 @@ TemporalWorkspace layoutTemporalWorkspace(const RestirParams* p, void* base)
 		offset += (bytes + 255u) & ~uint64_t(255u);
 		return start;
 	};
-	TemporalWorkspace w;
+	TemporalWorkspace w = {};
 	uint32_t* counters = reinterpret_cast<uint32_t*>(region(2 * sizeof(uint32_t)));
 	w.queue.count = counters;
 	w.queue.claimed = counters + 1;
@@ -709,6 +742,27 @@ TemporalWorkspace layoutTemporalWorkspace(const RestirParams* p, void* base)
 	w.records.slot = reinterpret_cast<int*>(region(n * 4));
 	w.queue.capacity = uint32_t(n);
 	w.records.candidates = p->initial_candidates;
+	if (p->radiance_cache > 0.5f)
+	{
+		CacheWorkspace& c = w.cache;
+		c.rows = uint32_t(n + uint64_t(p->gi_width) * p->gi_height);
+		c.queries = reinterpret_cast<float4*>(region(uint64_t(c.rows) * 64));
+		c.values = reinterpret_cast<uint16_t*>(region(uint64_t(c.rows) * 8));
+		c.samples = p->cache_training_samples;
+		const uint64_t s = c.samples;
+		c.trainQueue.rays = reinterpret_cast<float4*>(region(s * 32));
+		c.trainQueue.hitTriangle = reinterpret_cast<int*>(region(s * 4));
+		c.trainQueue.hitDistance = reinterpret_cast<float*>(region(s * 4));
+		c.trainQueue.claimed = reinterpret_cast<uint32_t*>(region(2 * sizeof(uint32_t)));
+		c.trainQueue.count = nullptr;
+		c.trainQueue.capacity = c.samples;
+		c.trainQueries = reinterpret_cast<float4*>(region(s * 64));
+		c.hitQueries = reinterpret_cast<float4*>(region(s * 64));
+		c.hitValues = reinterpret_cast<uint16_t*>(region(s * 8));
+		c.partial = reinterpret_cast<float4*>(region(s * 16));
+		c.hitAlbedo = reinterpret_cast<float4*>(region(s * 16));
+		c.targets = reinterpret_cast<float4*>(region(s * 16));
+	}
 	w.bytes = offset;
 	return w;
 }
@@ -734,6 +788,7 @@ int persistentBlocks()
 }
 
 } // namespace
+} // namespace restir
 
 extern "C" uint64_t restir_gi_temporal_workspace_bytes(const RestirParams* params)
 {
@@ -772,4 +827,347 @@ extern "C" int restir_gi_temporal_wavefront(const RestirParams* params, const Re
 	traceQueueKernel<<<persistentBlocks(), 128, 0, s>>>(bvh, w.queue);
 	giTemporalShadeKernel<<<blocks, kGiThreads, 0, s>>>(*params, bvh, b, w.records, w.queue);
 	return launchStatus();
+}
+
+// --- the radiance cache in the GI passes -----------------------------------------
+//
+// restir_gi_temporal_cached and restir_gi_spatial_cached are the GI passes
+// with the cache standing in for previousIndirect: before shading, one query
+// row per sample point the pass may shade (the candidates' hits, the reused
+// reservoirs' samples) is filled with the point's surface as evaluateSample
+// finds it, the cache answers all rows in one tensor-core launch, and the
+// shading reads the answers by slot. restir_cache_train_frame traces the
+// training batch: path suffixes from G-buffer points, each target the light
+// leaving the suffix's first hit, with the cache's own value there standing
+// for everything beyond it.
+
+namespace restir
+{
+namespace
+{
+
+__device__ __forceinline__ void writeQuery(float4* q, V3 position, float roughness, V3 normal, bool valid, V3 direction,
+	V3 albedo)
+{
+	q[0] = make_float4(position.x, position.y, position.z, roughness);
+	q[1] = make_float4(normal.x, normal.y, normal.z, valid ? 1.0f : 0.0f);
+	q[2] = make_float4(direction.x, direction.y, direction.z, 0.0f);
+	q[3] = make_float4(albedo.x, albedo.y, albedo.z, 0.0f);
+}
+
+// The query for a sample point shaded for a receiver: its surface as
+// evaluateSample finds it (restir.sh:466-495), the direction toward the
+// receiver; a padding row when the point is the sky or cannot be shaded.
+__device__ inline void sampleQuery(const GiPass& g, V3 receiver, V3 samplePosition, float sampleId, bool present, float4* q)
+{
+	bool visible = false;
+	V2 uv = v2(0.0f, 0.0f);
+	int triangle = -1;
+	V3 normal = v3(0.0f, 0.0f, 1.0f);
+	if (!present || isSkySample(sampleId) || !g.sampleSurface(samplePosition, sampleId, visible, uv, triangle, normal))
+	{
+		writeQuery(q, samplePosition, 0.0f, normal, false, normal, v3s(0.0f));
+		return;
+	}
+	const V3 albedo = visible ? g.diffuseAlbedo(uv) : g.bvh.albedo(triangle);
+	const float roughness = visible ? loadU8(g.albedoTex, g.full(uv)).w : 1.0f;
+	const V3 toReceiver = receiver - samplePosition;
+	const float distanceSquared = dot(toReceiver, toReceiver);
+	const V3 direction = distanceSquared > 0.0f ? toReceiver * inversesqrt(distanceSquared) : normal;
+	writeQuery(q, samplePosition, roughness, normal, true, direction, albedo);
+}
+
+// One row per candidate: its hit resolved as giTemporalShadeKernel resolves it.
+__global__ void __launch_bounds__(128) candidateQueryKernel(const RestirParams P, BvhView bvh, GiBindings b,
+	CandidateRecords records, RayQueue queue, float4* queries)
+{
+	const int r = int(blockIdx.x * blockDim.x + threadIdx.x);
+	const int w = int(P.gi_width), h = int(P.gi_height);
+	if (r >= w * h * records.candidates)
+	{
+		return;
+	}
+	GiPass g = makePass(P, bvh, b, P.prev_camera_position, nullptr, 0);
+	const int pixel = r / records.candidates;
+	const V2 uv = pixelUv(pixel % w, pixel / w, g.giTexel);
+	const float depth = g.depthAt(uv);
+	const V3 receiver = reconstructWorldPosition(P, uv, depth);
+	const float4 screen = records.screenHit[r];
+	const int slot = records.slot[r];
+	V3 hitPosition = v3(screen.x, screen.y, screen.z);
+	float hitId = 0.0f;
+	bool present = false;
+	if (slot >= 0)
+	{
+		const int triangle = queue.hitTriangle[slot];
+		if (triangle >= 0)
+		{
+			const float4 o = queue.rays[2 * slot];
+			const float4 d = queue.rays[2 * slot + 1];
+			const V3 direction = v3(d.x, d.y, d.z);
+			hitPosition = v3(o.x, o.y, o.z) + direction * queue.hitDistance[slot];
+			hitId = g.encodeSampleId(triangle, direction);
+			present = true;
+		}
+	}
+	else if (slot == -2)
+	{
+		present = screen.w > 0.5f;
+	}
+	sampleQuery(g, receiver, hitPosition, hitId, present && depth < kSkyDepth, queries + size_t(r) * 4);
+}
+
+// One row per reservoir of a GI-resolution set (last frame's, or this frame's
+// for the spatial pass).
+__global__ void __launch_bounds__(128) reservoirQueryKernel(const RestirParams P, BvhView bvh, GiBindings b,
+	const float4* sample, const float4* receiver, const float4* normal, float4* queries)
+{
+	const int i = int(blockIdx.x * blockDim.x + threadIdx.x);
+	if (i >= int(P.gi_width * P.gi_height))
+	{
+		return;
+	}
+	GiPass g = makePass(P, bvh, b, P.camera_position, nullptr, 0);
+	const float4 s = __ldg(sample + i);
+	const float4 r = __ldg(receiver + i);
+	const float4 n = __ldg(normal + i);
+	sampleQuery(g, v3(r.x, r.y, r.z), v3(s.x, s.y, s.z), n.w, s.w > 0.0f, queries + size_t(i) * 4);
+}
+
+// Training: sample j starts at a seeded GI pixel's G-buffer surface and
+// traces one cosine-distributed suffix ray.
+__global__ void __launch_bounds__(128) trainingRaysKernel(const RestirParams P, BvhView bvh, GiBindings b, CacheWorkspace c)
+{
+	const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= c.samples)
+	{
+		return;
+	}
+	GiPass g = makePass(P, bvh, b, P.camera_position, nullptr, 0);
+	const uint32_t pixels = P.gi_width * P.gi_height;
+	uint32_t rng = pcg(j + pcg(uint32_t(P.frame_index) ^ 0x2545f491u));
+	const uint32_t pixel = pcg(rng) % pixels;
+	const V2 uv = pixelUv(int(pixel % P.gi_width), int(pixel / P.gi_width), g.giTexel);
+	const float depth = g.depthAt(uv);
+	const bool valid = depth < kSkyDepth;
+	const V3 position = reconstructWorldPosition(P, uv, depth);
+	const V3 normal = g.decode(uv);
+	const float r0 = nextRandom(rng);
+	const float r1 = nextRandom(rng);
+	const V3 direction = GiPass::cosineHemisphere(normal, r0, r1);
+	const V3 origin = position + normal * g.kRayBias();
+	c.trainQueue.rays[2 * j] = make_float4(origin.x, origin.y, origin.z, valid ? g.kMaxBvhRayDistance() : 0.0f);
+	c.trainQueue.rays[2 * j + 1] = make_float4(direction.x, direction.y, direction.z, 0.0f);
+	const V3 camera = v3(P.camera_position[0], P.camera_position[1], P.camera_position[2]);
+	const V3 toCamera = camera - position;
+	const float distanceSquared = dot(toCamera, toCamera);
+	const V3 view = distanceSquared > 0.0f ? toCamera * inversesqrt(distanceSquared) : normal;
+	writeQuery(c.trainQueries + size_t(j) * 4, position, loadU8(g.albedoTex, g.full(uv)).w, normal, valid, view,
+		g.diffuseAlbedo(uv));
+}
+
+// The suffix's first hit: its direct light and emission now, a query for
+// the cache's value there.
+__global__ void __launch_bounds__(128) trainingHitsKernel(const RestirParams P, BvhView bvh, GiBindings b, CacheWorkspace c)
+{
+	const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= c.samples)
+	{
+		return;
+	}
+	GiPass g = makePass(P, bvh, b, P.camera_position, nullptr, 0);
+	const float weight = c.trainQueries[size_t(j) * 4 + 1].w;
+	const int triangle = c.trainQueue.hitTriangle[j];
+	const float4 o = c.trainQueue.rays[2 * j];
+	const float4 d = c.trainQueue.rays[2 * j + 1];
+	const V3 direction = v3(d.x, d.y, d.z);
+	V3 light = v3s(0.0f);
+	V3 albedo = v3s(0.0f);
+	float4* q = c.hitQueries + size_t(j) * 4;
+	if (weight > 0.0f && triangle >= 0)
+	{
+		const V3 hit = v3(o.x, o.y, o.z) + direction * c.trainQueue.hitDistance[j];
+		const float id = g.encodeSampleId(triangle, direction);
+		const V3 v0 = bvh.vertex(triangle, 0);
+		const V3 normal = normalize(cross(bvh.vertex(triangle, 1) - v0, bvh.vertex(triangle, 2) - v0)) * (id < 0.0f ? -1.0f : 1.0f);
+		albedo = bvh.albedo(triangle);
+		light = g.directFromLight(albedo, hit, normal) + bvh.emission(triangle) * P.emission_scale;
+		writeQuery(q, hit, 1.0f, normal, true, -direction, albedo);
+	}
+	else
+	{
+		if (weight > 0.0f && skyEnabled(P))
+		{
+			light = skyRadiance(P, direction);
+		}
+		writeQuery(q, v3s(0.0f), 0.0f, v3(0.0f, 0.0f, 1.0f), false, v3(0.0f, 0.0f, 1.0f), v3s(0.0f));
+	}
+	c.partial[j] = make_float4(light.x, light.y, light.z, weight);
+	c.hitAlbedo[j] = make_float4(albedo.x, albedo.y, albedo.z, 0.0f);
+}
+
+__global__ void __launch_bounds__(128) trainingTargetsKernel(CacheWorkspace c)
+{
+	const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= c.samples)
+	{
+		return;
+	}
+	const float4 partial = c.partial[j];
+	const float4 albedo = c.hitAlbedo[j];
+	const V4 cached = loadH4(c.hitValues, int(j));
+	const float beyond = cached.w > 0.5f ? 1.0f : 0.0f;
+	c.targets[j] = make_float4(partial.x + albedo.x * cached.x * beyond, partial.y + albedo.y * cached.y * beyond,
+		partial.z + albedo.z * cached.z * beyond, partial.w);
+}
+
+bool validCache(const RestirCacheConfig* cfg, const void* state)
+{
+	return cfg != nullptr && state != nullptr && (reinterpret_cast<uintptr_t>(state) & 255u) == 0u;
+}
+
+int gridFor(uint32_t n)
+{
+	return int((n + 127u) / 128u);
+}
+
+} // namespace
+} // namespace restir
+
+extern "C" int restir_gi_temporal_cached(const RestirParams* params, const RestirScene* scene, const RestirGBuffer* gbuffer,
+	const RestirGiHistory* history, const uint32_t* previous_grid, const float* shadow_atlas, const uint16_t* surface_light,
+	const RestirGiReservoirs* output, const RestirCacheConfig* cache_config, const void* cache_state, void* workspace,
+	uint64_t workspace_bytes, void* stream)
+{
+	if (!validCommon(params, scene, gbuffer, history, previous_grid, shadow_atlas) || history->sample == nullptr
+		|| output == nullptr || output->sample == nullptr || output->receiver == nullptr || output->normal == nullptr
+		|| workspace == nullptr || (reinterpret_cast<uintptr_t>(workspace) & 255u) != 0u || params->initial_candidates < 0
+		|| params->radiance_cache <= 0.5f || !validCache(cache_config, cache_state))
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	TemporalWorkspace w = layoutTemporalWorkspace(params, workspace);
+	if (workspace_bytes < w.bytes)
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	GiBindings b = bindings(gbuffer, history, previous_grid, shadow_atlas, surface_light);
+	b.outSample = reinterpret_cast<float4*>(output->sample);
+	b.outReceiver = reinterpret_cast<float4*>(output->receiver);
+	b.outNormal = reinterpret_cast<float4*>(output->normal);
+	const BvhView bvh = makeBvhView(scene);
+	cudaStream_t s = asStream(stream);
+	const int groups = int((params->gi_width + 3) / 4 * ((params->gi_height + 7) / 8));
+	const int blocks = (groups + kGiWarps - 1) / kGiWarps;
+	const uint32_t candidates = w.queue.capacity;
+	const uint32_t pixels = params->gi_width * params->gi_height;
+	cudaMemsetAsync(workspace, 0, 2 * sizeof(uint32_t), s);
+	giCandidatesKernel<<<blocks, kGiThreads, 0, s>>>(*params, bvh, b, w.records, w.queue);
+	traceQueueKernel<<<persistentBlocks(), 128, 0, s>>>(bvh, w.queue);
+	if (candidates > 0u)
+	{
+		candidateQueryKernel<<<gridFor(candidates), 128, 0, s>>>(*params, bvh, b, w.records, w.queue, w.cache.queries);
+	}
+	reservoirQueryKernel<<<gridFor(pixels), 128, 0, s>>>(*params, bvh, b, b.historySample, b.historyReceiver,
+		b.historyNormal, w.cache.queries + size_t(candidates) * 4);
+	int status = restir_cache_query(cache_config, cache_state, reinterpret_cast<const float*>(w.cache.queries), w.cache.rows,
+		w.cache.values, stream);
+	if (status != RESTIR_OK)
+	{
+		return status;
+	}
+	b.cache = w.cache.values;
+	b.cacheNeighbourBase = int(candidates);
+	giTemporalShadeKernel<<<blocks, kGiThreads, 0, s>>>(*params, bvh, b, w.records, w.queue);
+	return launchStatus();
+}
+
+extern "C" int restir_gi_spatial_cached(const RestirParams* params, const RestirScene* scene, const RestirGBuffer* gbuffer,
+	const RestirGiReservoirs* current, const uint32_t* current_grid, const RestirGiHistory* history, const float* shadow_atlas,
+	const uint16_t* surface_light, uint16_t* color, uint16_t* moments, const RestirCacheConfig* cache_config,
+	const void* cache_state, void* workspace, uint64_t workspace_bytes, void* stream)
+{
+	if (!validCommon(params, scene, gbuffer, history, current_grid, shadow_atlas) || current == nullptr
+		|| current->sample == nullptr || current->receiver == nullptr || current->normal == nullptr || color == nullptr
+		|| moments == nullptr || history->moments == nullptr || workspace == nullptr
+		|| (reinterpret_cast<uintptr_t>(workspace) & 255u) != 0u || params->radiance_cache <= 0.5f
+		|| !validCache(cache_config, cache_state))
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	TemporalWorkspace w = layoutTemporalWorkspace(params, workspace);
+	if (workspace_bytes < w.bytes)
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	GiBindings b = bindings(gbuffer, history, current_grid, shadow_atlas, surface_light);
+	b.reservoirSample = reinterpret_cast<const float4*>(current->sample);
+	b.reservoirReceiver = reinterpret_cast<const float4*>(current->receiver);
+	b.reservoirNormal = reinterpret_cast<const float4*>(current->normal);
+	b.outColor = color;
+	b.outMoments = moments;
+	const BvhView bvh = makeBvhView(scene);
+	cudaStream_t s = asStream(stream);
+	const uint32_t pixels = params->gi_width * params->gi_height;
+	reservoirQueryKernel<<<gridFor(pixels), 128, 0, s>>>(*params, bvh, b, b.reservoirSample, b.reservoirReceiver,
+		b.reservoirNormal, w.cache.queries);
+	int status = restir_cache_query(cache_config, cache_state, reinterpret_cast<const float*>(w.cache.queries), pixels,
+		w.cache.values, stream);
+	if (status != RESTIR_OK)
+	{
+		return status;
+	}
+	b.cache = w.cache.values;
+	b.cacheNeighbourBase = 0;
+	dim3 grid((params->gi_width + 15) / 16, (params->gi_height + 7) / 8);
+	giSpatialKernel<<<grid, 128, 0, s>>>(*params, bvh, b);
+	return launchStatus();
+}
+
+extern "C" int restir_cache_train_frame(const RestirParams* params, const RestirScene* scene, const RestirGBuffer* gbuffer,
+	const float* shadow_atlas, const RestirCacheConfig* cache_config, void* cache_state, void* workspace,
+	uint64_t workspace_bytes, void* stream)
+{
+	if (params == nullptr || scene == nullptr || gbuffer == nullptr || shadow_atlas == nullptr || gbuffer->albedo == nullptr
+		|| gbuffer->normal == nullptr || gbuffer->depth == nullptr || workspace == nullptr
+		|| (reinterpret_cast<uintptr_t>(workspace) & 255u) != 0u || params->radiance_cache <= 0.5f
+		|| params->gi_width == 0u || params->gi_height == 0u || !validCache(cache_config, cache_state))
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	TemporalWorkspace w = layoutTemporalWorkspace(params, workspace);
+	if (workspace_bytes < w.bytes)
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	const CacheWorkspace& c = w.cache;
+	if (c.samples == 0u)
+	{
+		return RESTIR_OK;
+	}
+	GiBindings b = {};
+	b.albedo = gbuffer->albedo;
+	b.normal = gbuffer->normal;
+	b.depth = gbuffer->depth;
+	b.shadowAtlas = shadow_atlas;
+	const BvhView bvh = makeBvhView(scene);
+	cudaStream_t s = asStream(stream);
+	cudaMemsetAsync(c.trainQueue.claimed, 0, sizeof(uint32_t), s);
+	trainingRaysKernel<<<gridFor(c.samples), 128, 0, s>>>(*params, bvh, b, c);
+	traceQueueKernel<<<persistentBlocks(), 128, 0, s>>>(bvh, c.trainQueue);
+	trainingHitsKernel<<<gridFor(c.samples), 128, 0, s>>>(*params, bvh, b, c);
+	int status = restir_cache_query(cache_config, cache_state, reinterpret_cast<const float*>(c.hitQueries), c.samples,
+		c.hitValues, stream);
+	if (status != RESTIR_OK)
+	{
+		return status;
+	}
+	trainingTargetsKernel<<<gridFor(c.samples), 128, 0, s>>>(c);
+	status = launchStatus();
+	if (status != RESTIR_OK)
+	{
+		return status;
+	}
+	return restir_cache_train(cache_config, cache_state, reinterpret_cast<const float*>(c.trainQueries),
+		reinterpret_cast<const float*>(c.targets), c.samples, stream);
 }

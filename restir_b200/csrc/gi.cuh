@@ -59,6 +59,7 @@ struct NeighbourReservoir
 	V3 receiverNormal;
 	float count;
 	float weight;
+	int cacheSlot;  // the radiance cache's value for this sample, or -1
 };
 
 struct PairwiseMis
@@ -203,6 +204,11 @@ struct GiPass
 	int stackStride;
 	int W, H, w, h;
 	V2 giSize, giTexel;
+	// Radiance-cache values (half4: irradiance, valid) indexed by a slot, in
+	// place of previousIndirect when P.radiance_cache is set; reused
+	// neighbours' samples sit at cacheNeighbourBase + their pixel index.
+	const uint16_t* cache;
+	int cacheNeighbourBase;
 
 	__device__ __forceinline__ float s() const { return P.scene_scale; }
 	__device__ __forceinline__ float kRayBias() const { return 0.02f * s(); }
@@ -433,20 +439,14 @@ struct GiPass
 		return false;
 	}
 
-	__device__ inline bool evaluateSample(V3 receiverPosition, V3 receiverNormal, V3 receiverAlbedo, V3 samplePosition,
-		float sampleId, V3& contribution, V3& sampleNormal) const
+	// The surface a (non-sky) sample lies on, as evaluateSample shades it
+	// (restir.sh:466-495): the visible surface from the G-buffer when the
+	// sample projects onto it, else its triangle from the BVH. False when
+	// neither holds.
+	__device__ inline bool sampleSurface(V3 samplePosition, float sampleId, bool& visibleSurface, V2& sampleUv,
+		int& triangleIndex, V3& sampleNormal) const
 	{
-		contribution = v3s(0.0f);
-		sampleNormal = v3(0.0f, 0.0f, 1.0f);
-		if (isSkySample(sampleId))
-		{
-			sampleNormal = -samplePosition;
-			contribution = receiverAlbedo * skyRadiance(P, samplePosition)
-				* (fmaxf(dot(receiverNormal, samplePosition), 0.0f) / kPi);
-			return skyEnabled(P);
-		}
-		bool visibleSurface = false;
-		V2 sampleUv;
+		visibleSurface = false;
 		float sampleViewDepth;
 		if (projectToScreen(samplePosition, sampleUv, sampleViewDepth))
 		{
@@ -454,7 +454,7 @@ struct GiPass
 			visibleSurface = sampleDepth < kSkyDepth
 				&& distance(reconstructWorldPosition(P, sampleUv, sampleDepth), samplePosition) <= kSampleTolerance();
 		}
-		int triangleIndex = int(fabsf(sampleId) + 0.5f) - 1;
+		triangleIndex = int(fabsf(sampleId) + 0.5f) - 1;
 		if (!visibleSurface && (triangleIndex < 0 || !bvh.available()))
 		{
 			return false;
@@ -468,6 +468,40 @@ struct GiPass
 			V3 v0 = bvh.vertex(triangleIndex, 0);
 			sampleNormal = normalize(cross(bvh.vertex(triangleIndex, 1) - v0, bvh.vertex(triangleIndex, 2) - v0))
 				* (sampleId < 0.0f ? -1.0f : 1.0f);
+		}
+		return true;
+	}
+
+	// Indirect light leaving the sample point: the radiance cache's value when
+	// one is given, else previousIndirect.
+	__device__ __forceinline__ V3 sampleIndirect(V3 p, V3 n, V3 albedo, int cacheSlot) const
+	{
+		if (cache != nullptr && cacheSlot >= 0)
+		{
+			V4 cached = loadH4(cache, cacheSlot);
+			return cached.w > 0.5f ? cached.xyz() * albedo : v3s(0.0f);
+		}
+		return previousIndirect(p, n, albedo);
+	}
+
+	__device__ inline bool evaluateSample(V3 receiverPosition, V3 receiverNormal, V3 receiverAlbedo, V3 samplePosition,
+		float sampleId, V3& contribution, V3& sampleNormal, int cacheSlot = -1) const
+	{
+		contribution = v3s(0.0f);
+		sampleNormal = v3(0.0f, 0.0f, 1.0f);
+		if (isSkySample(sampleId))
+		{
+			sampleNormal = -samplePosition;
+			contribution = receiverAlbedo * skyRadiance(P, samplePosition)
+				* (fmaxf(dot(receiverNormal, samplePosition), 0.0f) / kPi);
+			return skyEnabled(P);
+		}
+		bool visibleSurface;
+		V2 sampleUv;
+		int triangleIndex;
+		if (!sampleSurface(samplePosition, sampleId, visibleSurface, sampleUv, triangleIndex, sampleNormal))
+		{
+			return false;
 		}
 		V3 toReceiver = receiverPosition - samplePosition;
 		float distanceSquared = dot(toReceiver, toReceiver);
@@ -487,14 +521,14 @@ struct GiPass
 		{
 			V3 albedo = diffuseAlbedo(sampleUv);
 			radiance = directFromLight(albedo, samplePosition, sampleNormal)
-				+ previousIndirect(samplePosition, sampleNormal, albedo)
+				+ sampleIndirect(samplePosition, sampleNormal, albedo, cacheSlot)
 				+ loadH4(surfaceLight, full(sampleUv)).xyz() * P.surface_light_scale;
 		}
 		else
 		{
 			V3 albedo = bvh.albedo(triangleIndex);
 			radiance = directFromLight(albedo, samplePosition, sampleNormal)
-				+ previousIndirect(samplePosition, sampleNormal, albedo)
+				+ sampleIndirect(samplePosition, sampleNormal, albedo, cacheSlot)
 				+ bvh.emission(triangleIndex) * P.emission_scale;
 		}
 		contribution = receiverAlbedo * radiance * (receiverCosine / kPi);
@@ -583,6 +617,7 @@ struct GiPass
 		nb.receiverNormal = v3(0.0f, 0.0f, 1.0f);
 		nb.count = fminf(sample.w, 20.0f);
 		nb.weight = receiver.w;
+		nb.cacheSlot = -1;
 		V3 rn = receiverNormal.xyz();
 		if (sample.w <= 0.0f || dot(rn, rn) < 0.5f)
 		{
@@ -647,7 +682,7 @@ struct GiPass
 		bool shifted = false;
 		if (nb.weight > 0.0f)
 		{
-			shifted = evaluateSample(p, n, albedo, nb.samplePosition, nb.sampleId, contribution, sampleNormal);
+			shifted = evaluateSample(p, n, albedo, nb.samplePosition, nb.sampleId, contribution, sampleNormal, nb.cacheSlot);
 		}
 		if (shifted)
 		{

@@ -1,6 +1,7 @@
 // The uniforms of one frame, as Renderer::render derives them
 // (src/renderer.cpp:435-731), and the state it carries to the next
 // (renderer.cpp:1119-1124).
+#include "../../include/restir_cache.h"
 #include "../../include/restir_frame.h"
 #include "bvh_build.h"
 
@@ -81,6 +82,8 @@ extern "C" void restir_settings_default(RestirSettings* s)
 	s->grid_cell_capacity = 32;
 	s->grid_mode = RESTIR_GRID_ATOMIC;
 	s->wavefront = 1;
+	s->radiance_cache = 0;
+	s->cache_training_samples = 65536;
 }
 
 extern "C" int restir_frame_params(const RestirSettings* requested, const RestirMeshDesc* scene, uint32_t light_count,
@@ -188,6 +191,11 @@ extern "C" int restir_frame_params(const RestirSettings* requested, const Restir
 	p->grid_cell_capacity = s.grid_cell_capacity;
 	p->grid_mode = s.grid_mode;
 	p->ray_mode = s.ray_mode;
+	// The radiance cache replaces the history-based bounce; reference
+	// accumulation keeps the plain method.
+	p->radiance_cache = (s.radiance_cache && s.wavefront && !state->reference_accumulating) ? 1.0f : 0.0f;
+	p->cache_training_samples = s.cache_training_samples < RESTIR_CACHE_MAX_BATCH ? s.cache_training_samples
+		: RESTIR_CACHE_MAX_BATCH;
 
 	// The shadow atlas (renderer.cpp:527-593): six faces of a slightly wider
 	// field of view than 90 degrees, a border of 4 texels.

@@ -49,9 +49,10 @@ public:
 		cudaStreamCreateWithFlags(&m_stream, cudaStreamNonBlocking);
 		for (auto& frame : m_events)
 		{
-			for (cudaEvent_t& e : frame)
+			for (auto& pass : frame)
 			{
-				cudaEventCreate(&e);
+				cudaEventCreate(&pass[0]);
+				cudaEventCreate(&pass[1]);
 			}
 		}
 		cudaMallocHost(&m_errorHost, 4 * sizeof(double));
@@ -65,9 +66,10 @@ public:
 		releaseScene();
 		for (auto& frame : m_events)
 		{
-			for (cudaEvent_t& e : frame)
+			for (auto& pass : frame)
 			{
-				cudaEventDestroy(e);
+				cudaEventDestroy(pass[0]);
+				cudaEventDestroy(pass[1]);
 			}
 		}
 		cudaFreeHost(m_errorHost);
@@ -212,7 +214,7 @@ public:
 			ms[i] = 0.0f;
 			if (m_timed && m_passRan[m_lastSlot][i])
 			{
-				cudaEventElapsedTime(&ms[i], m_events[m_lastSlot][i], m_events[m_lastSlot][i + 1]);
+				cudaEventElapsedTime(&ms[i], m_events[m_lastSlot][i][0], m_events[m_lastSlot][i][1]);
 			}
 		}
 	}
@@ -234,7 +236,7 @@ public:
 				float t = 0.0f;
 				if (m_passRan[slot][i])
 				{
-					cudaEventElapsedTime(&t, m_events[slot][i], m_events[slot][i + 1]);
+					cudaEventElapsedTime(&t, m_events[slot][i][0], m_events[slot][i][1]);
 				}
 				ms[f * RESTIR_PASS_COUNT + i] = t;
 			}
@@ -472,11 +474,11 @@ private:
 			&& P.grid_cell_capacity == m_capacity;
 	}
 
-	void mark(int pass, bool events)
+	void mark(int pass, int edge, bool events)
 	{
 		if (events)
 		{
-			cudaEventRecord(m_events[m_slot][pass], m_stream);
+			cudaEventRecord(m_events[m_slot][pass][edge], m_stream);
 		}
 	}
 
@@ -507,10 +509,10 @@ private:
 		}
 		auto run = [&](int pass, auto&& body)
 		{
-			mark(pass, events);
+			mark(pass, 0, events);
 			status |= body();
 			m_passRan[m_slot][pass] = true;
-			mark(pass + 1, events);
+			mark(pass, 1, events);
 			if (m_profile != nullptr)
 			{
 				// restir_counters waits for the device: this pass's work only.
@@ -675,7 +677,7 @@ private:
 	// Per-pass events of the last kEventRing stream-launched frames.
 	static constexpr uint32_t kEventRing = 128;
 	bool m_passRan[kEventRing][RESTIR_PASS_COUNT] = {};
-	cudaEvent_t m_events[kEventRing][RESTIR_PASS_COUNT + 1] = {};
+	cudaEvent_t m_events[kEventRing][RESTIR_PASS_COUNT][2] = {};  // start, end of each pass
 	uint32_t m_slot = 0;
 	uint32_t m_lastSlot = 0;
 	uint32_t m_timedFrames = 0;

@@ -79,6 +79,7 @@ def test_oracle_gradients_against_numpy():
     q[:, 8:11] = rng.normal(size=(n, 3))
     q[:, 12:15] = rng.uniform(0, 1, (n, 3))
     targets = rng.uniform(0.1, 1.0, (n, 4)).astype(np.float32)
+    targets[:, 3] = 1.0
     feats = np.zeros((n, 64), np.uint16)
     lib = ob.load()
     lib.oracle_cache_features(C.byref(cfg), C.byref(layout), table.ctypes.data, q.ctypes.data, n, feats.ctypes.data)

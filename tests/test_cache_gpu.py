@@ -24,6 +24,7 @@ def make_queries(n, seed=0, lo=(-2.0, -1.0, -3.0), hi=(2.0, 3.0, 1.0)):
         v = rng.normal(size=(n, 3))
         q[:, col:col + 3] = v / np.linalg.norm(v, axis=1, keepdims=True)
     q[:, 12:15] = rng.uniform(0.05, 0.95, (n, 3))
+    q[:, 7] = 1.0  # valid
     return q
 
 
@@ -31,6 +32,7 @@ def target_function(q):
     """A smooth positive radiance over position and normal."""
     p = q[:, 0:3]
     t = np.zeros((len(q), 4), np.float32)
+    t[:, 3] = 1.0  # weight
     t[:, 0] = 0.6 + 0.4 * np.sin(2.0 * p[:, 0]) * np.cos(1.5 * p[:, 1])
     t[:, 1] = 0.5 + 0.3 * q[:, 5] + 0.1 * np.sin(3.0 * p[:, 2])
     t[:, 2] = 0.3 + 0.2 * np.cos(p[:, 0] + p[:, 2])
@@ -90,10 +92,11 @@ def test_forward_matches_oracle(trained, n):
     np.testing.assert_allclose(got[:, :3], want[:, :3], rtol=2e-2, atol=2e-2 * scale)
     # The padding outputs have zero weights.
     assert np.all(got[:, 3:] == 0.0)
-    # query() is max(output, 0) as half, alpha 1.
-    h = trained.query(dq).cpu().numpy().astype(np.float32)
+    # query() is max(output, 0) as half, alpha the query's valid flag.
+    q[::2, 7] = 0.0
+    h = trained.query(torch.from_numpy(q).cuda()).cpu().numpy().astype(np.float32)
     np.testing.assert_allclose(h[:, :3], np.maximum(got[:, :3], 0.0), rtol=1e-3, atol=1e-4)
-    assert np.all(h[:, 3] == 1.0)
+    np.testing.assert_array_equal(h[:, 3], q[:, 7])
 
 
 @pytest.mark.gpu
@@ -102,6 +105,7 @@ def test_gradients_match_oracle(trained, n):
     import torch
     q = make_queries(n, seed=3)
     t = target_function(q)
+    t[::3, 3] = 0.0  # samples of weight 0 drop out of the loss and the gradients
     weights = host_region(trained, "weights_bf16", torch.int16).view(np.uint16).copy()
     table = host_region(trained, "table_half", torch.int16).view(np.uint16).copy()
     scale = trained.scalars().loss_scale

@@ -69,6 +69,28 @@ def test_gi_temporal_wavefront_bit_exact(case):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("case", ["cornell", "courtyard", "bvh-rays"])
+def test_gi_passes_with_radiance_cache_bit_exact(case):
+    """With the radiance cache standing in for previousIndirect, the GI passes
+    reproduce the oracle's outputs bit for bit given the same cache values
+    (the oracle reads the values the CUDA pass's queries returned); the cache
+    trains every frame on path suffixes."""
+    c, setup, settings = _case_setup(case)
+    settings.radiance_cache = 1
+    settings.cache_training_samples = 4096
+    w, h = c["size"]
+    rb.status_flags()
+    report, oracle_run, cuda_run = run_checked(setup, w, h, c["frames"] + 1, settings)
+    assert report == {}, report
+    s = cuda_run.cache.scalars()
+    assert s.step == c["frames"] + 1 and s.samples == 4096 and s.skipped_steps == 0
+    values = oracle_run.cache_values.reshape(-1, 4)
+    live = values[:, 3] == 0x3C00  # half 1.0: rows that were queries
+    assert live.sum() > 0.2 * len(values)
+    assert rb.status_flags() & (4 | 8) == 0
+
+
+@pytest.mark.gpu
 def test_gi_temporal_wavefront_rejects_bad_workspace():
     import torch
     setup = make_scene(rb.SCENE_CORNELL)
