@@ -45,6 +45,12 @@ WIDTH, HEIGHT = 1920, 1080
 TRIANGLES = 1_000_000
 EXTRA_LIGHTS = 64
 REFERENCE_FRAMES = 64
+ERROR_FRAMES = 30          # frames the relMSE is averaged over
+# DRAM bytes (read + write) per frame of a pass's kernels, from the committed ncu capture of this
+# workload (profiles/gi_temporal_wavefront_1080p_city1M.md): candidates 15.9 MB, queue tracer
+# 30.7 MB, shading 83.9 MB.
+DOMINANT_TRAFFIC = {"gi_temporal": 130.5e6}
+CACHE_TRAIN_FRAMES = 60    # online training before the radiance-cache form is timed
 
 # Algorithmic (compulsory) bytes per pixel of each pass's image reads and
 # writes, besides its BVH traversal (32 B per node fetch, 48 B per triangle
@@ -192,6 +198,48 @@ def reference_arm(args, rank: int, world: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def error_stats(renderer, frame, frames: int) -> dict:
+    """relMSE of the live image against the FP64 reference over `frames` frames."""
+    values = []
+    for _ in range(frames):
+        renderer.render(frame)
+        values.append(renderer.frame_submitted().relative_mse)
+    return {"mean": float(np.mean(values)), "median": float(np.median(values))}
+
+
+def cache_arm(renderer, frame, steps: int) -> dict:
+    """The radiance-cache form on the same view: CACHE_TRAIN_FRAMES frames of
+    online training, then `steps` timed frames (CUDA events on the renderer's
+    stream) and the relMSE over ERROR_FRAMES frames."""
+    import torch
+    import restir_b200 as rb
+    settings = renderer.settings
+    settings.radiance_cache = 1
+    renderer.settings = settings
+    for _ in range(CACHE_TRAIN_FRAMES):
+        renderer.render(frame)
+    renderer.synchronize()
+    stream = torch.cuda.ExternalStream(renderer.stream)
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record(stream)
+    for _ in range(steps):
+        renderer.render(frame)
+    stop.record(stream)
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(stop) / steps
+    pass_ms = renderer.pass_history(steps)
+    mean_pass = pass_ms.mean(axis=0) if len(pass_ms) else np.zeros(len(rb.PASS_NAMES))
+    error = error_stats(renderer, frame, ERROR_FRAMES)
+    params, _, _ = renderer.last_frame()
+    settings.radiance_cache = 0
+    renderer.settings = settings
+    return {"ms_per_frame": ms, "rel_mse_vs_fp64_reference": error["mean"], "rel_mse_median": error["median"],
+            "training_frames": CACHE_TRAIN_FRAMES + steps, "training_samples_per_frame": int(params.cache_training_samples),
+            "pass_ms": {name: float(mean_pass[i]) for i, name in enumerate(rb.PASS_NAMES)}}
+
+
 def own_arm(args, rank: int, world: int) -> None:
     import torch
 
@@ -271,6 +319,12 @@ def own_arm(args, rank: int, world: int) -> None:
         step_metrics = renderer.frame_submitted()
     e2e_ms = (time.perf_counter() - t) * 1e3 / args.steps
 
+    # relMSE against the FP64 reference over several frames (one frame's value
+    # swings with the fireflies of the specular DI), then the same for the
+    # radiance-cache form after it has trained.
+    plain_error = error_stats(renderer, frame, ERROR_FRAMES)
+    cache_line = cache_arm(renderer, frame, args.steps) if not args.no_cache else None
+
     total = torch.tensor([elapsed_ms, e2e_ms], device="cuda", dtype=torch.float64)
     if dist is not None:
         dist.all_reduce(total, op=dist.ReduceOp.MAX)
@@ -287,7 +341,7 @@ def own_arm(args, rank: int, world: int) -> None:
     passes = rb.PASS_NAMES
     mean_pass = pass_ms.mean(axis=0) if len(pass_ms) else np.zeros(len(passes))
     sizes = {"full": WIDTH * HEIGHT, "gi": params.gi_width * params.gi_height,
-             "atlas": 6 * params.shadow_face_size ** 2}
+             "atlas": 6 * params.shadow_face_size ** 2, "none": 0}
     pass_bytes = {}
     for i, name in enumerate(passes):
         res, per_pixel = PASS_PIXEL_BYTES[name]
@@ -318,8 +372,10 @@ def own_arm(args, rank: int, world: int) -> None:
         "mrays_per_s": float(rays / (ms_per_frame * 1e-3) / 1e6),
         "rays_per_frame": {"primary_and_shadow_map": int(counts[:, 0].sum()), "gi_closest": int(counts[:, 1].sum()),
                            "visibility_any_hit": int(counts[:, 2].sum()), "depth_buffer_marches": int(counts[:, 3].sum())},
-        "rel_mse_vs_fp64_reference": metrics.relative_mse, "bias_vs_fp64_reference": metrics.bias,
+        "rel_mse_vs_fp64_reference": plain_error["mean"], "rel_mse_median": plain_error["median"],
+        "bias_vs_fp64_reference": metrics.bias, "rel_mse_frames": ERROR_FRAMES,
         "reference_frames": REFERENCE_FRAMES,
+        "radiance_cache": cache_line,
         "pass_ms": {name: float(mean_pass[i]) for i, name in enumerate(passes)},
         "pass_share": share,
         "pass_algorithmic_gbs": {name: (float(pass_bytes[name] / (mean_pass[i] * 1e-3) / 1e9) if mean_pass[i] > 0 else 0.0)
@@ -332,7 +388,10 @@ def own_arm(args, rank: int, world: int) -> None:
         "gpu_launches": launches * args.steps,
         "roofline": {"bound": "hbm", "kernel": passes[dominant], "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                     "traffic": None, "algorithmic_bytes_per_launch": pass_bytes[passes[dominant]]},
+                     "traffic": DOMINANT_TRAFFIC.get(passes[dominant]),
+                     "traffic_source": "profiles/gi_temporal_wavefront_1080p_city1M.md (ncu DRAM read+write of the "
+                                       "pass's kernels, one cold launch each)",
+                     "algorithmic_bytes_per_launch": pass_bytes[passes[dominant]]},
         "cpu_baseline": baseline,
         "clocks": clocks,
     }
@@ -350,6 +409,7 @@ def main():
     parser.add_argument("--impl", default="own", choices=["own", "reference"])
     parser.add_argument("--graph", action="store_true", help="replay each frame as a CUDA graph")
     parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--no-cache", action="store_true", help="skip the radiance-cache form's measurement")
     parser.add_argument("--quick", action="store_true",
                         help="profiling runs: W + K frames of the workload, no reference, no report")
     args = parser.parse_args()

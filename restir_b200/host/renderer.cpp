@@ -8,6 +8,7 @@
 // stream capture and replays it as one CUDA graph launch; later frames are
 // captured again and patched into the instantiated graph
 // (cudaGraphExecUpdate), since their uniforms and ping-pong buffers change.
+#include "../../include/restir_cache.h"
 #include "../../include/restir_frame.h"
 #include "bvh_build.h"
 
@@ -93,11 +94,33 @@ public:
 		status |= upload(m_sceneBuffers["materials"], mesh.materialData.data(), mesh.materialData.size() * sizeof(float));
 		m_lightsKey.clear();
 		status |= updateLights();
+		status |= initCache(mesh);
 		m_state.history_valid = 0;
 		m_state.di_valid = 0;
 		m_state.reference_frames = 0;
 		m_hasScene = status == 0;
 		return status == 0 ? RESTIR_OK : RESTIR_ERROR_OUT_OF_MEMORY;
+	}
+
+	// The radiance cache over the scene's box (1% of the radius wider), fresh
+	// for every scene.
+	int initCache(const Mesh& mesh)
+	{
+		restir_cache_config_default(&m_cacheConfig);
+		for (int i = 0; i < 3; ++i)
+		{
+			m_cacheConfig.bounds_min[i] = mesh.boundsMin[i] - 0.01f * mesh.radius;
+			m_cacheConfig.bounds_max[i] = mesh.boundsMax[i] + 0.01f * mesh.radius;
+		}
+		const uint64_t bytes = restir_cache_state_bytes(&m_cacheConfig);
+		Buffer& b = m_sceneBuffers["cache.state"];
+		b.bytes = bytes;
+		if (bytes == 0 || cudaMalloc(&b.pointer, bytes) != cudaSuccess)
+		{
+			b.pointer = nullptr;
+			return 1;
+		}
+		return restir_cache_init(&m_cacheConfig, b.pointer, m_stream) == RESTIR_OK ? 0 : 1;
 	}
 
 	int setSettings(const RestirSettings& settings)
@@ -545,10 +568,17 @@ private:
 		RestirGiHistory history = { p<float>("gi.sample" + R), p<float>("gi.receiver" + R), p<float>("gi.normal" + R),
 			plan.denoiser ? p<uint16_t>("filtered" + R) : p<uint16_t>("gi.color" + R), p<uint16_t>("gi.moments" + R) };
 		RestirGiReservoirs current = { p<float>("gi.sample" + H), p<float>("gi.receiver" + H), p<float>("gi.normal" + H) };
+		const bool cached = P.radiance_cache > 0.5f;
+		void* cacheState = m_sceneBuffers["cache.state"].pointer;
 		run(RESTIR_PASS_GI_TEMPORAL, [&] {
+			const Buffer& w = m_targets["gi.workspace"];
+			if (cached)
+			{
+				return restir_gi_temporal_cached(&P, &scene, &gb, &history, p<uint32_t>("grid" + R), p<float>("shadow.atlas"),
+					surface, &current, &m_cacheConfig, cacheState, w.pointer, w.bytes, s);
+			}
 			if (m_settings.wavefront)
 			{
-				const Buffer& w = m_targets["gi.workspace"];
 				return restir_gi_temporal_wavefront(&P, &scene, &gb, &history, p<uint32_t>("grid" + R), p<float>("shadow.atlas"),
 					surface, &current, w.pointer, w.bytes, s);
 			}
@@ -556,9 +586,24 @@ private:
 				&current, s);
 		});
 		run(RESTIR_PASS_GI_SPATIAL, [&] {
+			if (cached)
+			{
+				const Buffer& w = m_targets["gi.workspace"];
+				return restir_gi_spatial_cached(&P, &scene, &gb, &current, gridWrite, &history, p<float>("shadow.atlas"), surface,
+					p<uint16_t>("gi.color" + H), p<uint16_t>("gi.moments" + H), &m_cacheConfig, cacheState, w.pointer, w.bytes, s);
+			}
 			return restir_gi_spatial(&P, &scene, &gb, &current, gridWrite, &history, p<float>("shadow.atlas"), surface,
 				p<uint16_t>("gi.color" + H), p<uint16_t>("gi.moments" + H), s);
 		});
+		if (cached)
+		{
+			// Training after the frame's queries: every query of a frame sees the same weights.
+			run(RESTIR_PASS_CACHE, [&] {
+				const Buffer& w = m_targets["gi.workspace"];
+				return restir_cache_train_frame(&P, &scene, &gb, p<float>("shadow.atlas"), &m_cacheConfig, cacheState, w.pointer,
+					w.bytes, s);
+			});
+		}
 		std::string denoised = "gi.color" + H;
 		if (plan.denoiser)
 		{
@@ -678,6 +723,7 @@ private:
 	static constexpr uint32_t kEventRing = 128;
 	bool m_passRan[kEventRing][RESTIR_PASS_COUNT] = {};
 	cudaEvent_t m_events[kEventRing][RESTIR_PASS_COUNT][2] = {};  // start, end of each pass
+	RestirCacheConfig m_cacheConfig = {};
 	uint32_t m_slot = 0;
 	uint32_t m_lastSlot = 0;
 	uint32_t m_timedFrames = 0;
