@@ -198,6 +198,66 @@ def reference_arm(args, rank: int, world: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def cache_kernels(args) -> None:
+    """--cache-kernels: the radiance cache's kernels alone on seeded synthetic
+    queries (the frame's query count, 2,073,600, and a 65,536-sample training
+    batch), timed with CUDA events; for profiling the tcgen05 MLP."""
+    import torch
+    import restir_b200 as rb
+    rng = np.random.default_rng(1)
+
+    def queries(n):
+        q = np.zeros((n, 16), np.float32)
+        q[:, 0:3] = rng.uniform(-1.0, 1.0, (n, 3))
+        q[:, 3] = rng.uniform(0.0, 1.0, n)
+        for col in (4, 8):
+            v = rng.normal(size=(n, 3))
+            q[:, col:col + 3] = v / np.linalg.norm(v, axis=1, keepdims=True)
+        q[:, 7] = 1.0
+        q[:, 12:15] = rng.uniform(0.05, 0.95, (n, 3))
+        return torch.from_numpy(q).cuda()
+
+    cache = rb.RadianceCache(rb.cache_config(bounds_min=(-1.0, -1.0, -1.0), bounds_max=(1.0, 1.0, 1.0)))
+    frame_queries = queries(2_073_600)
+    train_queries = queries(65536)
+    targets = torch.rand((65536, 4), device="cuda")
+    targets[:, 3] = 1.0
+    out = torch.empty((frame_queries.shape[0], 4), dtype=torch.float16, device="cuda")
+    for _ in range(args.warmup):
+        cache.query(frame_queries, out)
+        cache.train(train_queries, targets)
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(args.steps):
+        cache.query(frame_queries, out)
+    stop.record()
+    torch.cuda.synchronize()
+    query_ms = start.elapsed_time(stop) / args.steps
+    start.record()
+    for _ in range(args.steps):
+        cache.train(train_queries, targets)
+    stop.record()
+    torch.cuda.synchronize()
+    train_ms = start.elapsed_time(stop) / args.steps
+    flops = 2 * (64 * 64 * 4 + 16 * 64) * frame_queries.shape[0]
+    print(json.dumps({"cache_kernels": True, "query_ms": query_ms, "queries": int(frame_queries.shape[0]),
+                      "query_tflops": flops / (query_ms * 1e-3) / 1e12, "train_ms": train_ms,
+                      "training_samples": 65536, "loss": cache.scalars().loss,
+                      "status": rb.status_flags()}), flush=True)
+
+
+def max_over_ranks(values, dist, device: str) -> list:
+    """Every rank's timings reduced to the maximum over the ranks (the job's
+    time is its slowest replica's); every rank must call it. dist None: one
+    process."""
+    import torch
+    total = torch.tensor(values, device=device, dtype=torch.float64)
+    if dist is not None:
+        dist.all_reduce(total, op=dist.ReduceOp.MAX)
+    return [float(v) for v in total]
+
+
 def error_stats(renderer, frame, frames: int) -> dict:
     """relMSE of the live image against the FP64 reference over `frames` frames."""
     values = []
@@ -325,10 +385,7 @@ def own_arm(args, rank: int, world: int) -> None:
     plain_error = error_stats(renderer, frame, ERROR_FRAMES)
     cache_line = cache_arm(renderer, frame, args.steps) if not args.no_cache else None
 
-    total = torch.tensor([elapsed_ms, e2e_ms], device="cuda", dtype=torch.float64)
-    if dist is not None:
-        dist.all_reduce(total, op=dist.ReduceOp.MAX)
-    elapsed_ms, e2e_ms = float(total[0]), float(total[1])
+    elapsed_ms, e2e_ms = max_over_ranks([elapsed_ms, e2e_ms], dist, "cuda")
     if rank != 0:
         renderer.close()
         if dist is not None:
@@ -410,13 +467,17 @@ def main():
     parser.add_argument("--graph", action="store_true", help="replay each frame as a CUDA graph")
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--no-cache", action="store_true", help="skip the radiance-cache form's measurement")
+    parser.add_argument("--cache-kernels", action="store_true",
+                        help="time the radiance cache's query and training kernels alone (profiling)")
     parser.add_argument("--quick", action="store_true",
                         help="profiling runs: W + K frames of the workload, no reference, no report")
     args = parser.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.gpus == 1 else 1)))
-    if args.impl == "reference":
+    if args.cache_kernels:
+        cache_kernels(args)
+    elif args.impl == "reference":
         reference_arm(args, rank, world)
     else:
         own_arm(args, rank, world)
