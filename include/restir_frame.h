@@ -67,6 +67,8 @@ typedef struct RestirSettings
 	                            sample points from the radiance cache (restir_cache.h),
 	                            trained every frame; needs wavefront */
 	uint32_t cache_training_samples;  /* path suffixes per frame (default 65,536) */
+	uint32_t wave_visibility;         /* 1: visibility rays in warp lock step (traceBvhWave,
+	                                     bvh.sh:177-212, the reference's Vulkan path) */
 } RestirSettings;
 
 /* FrameInput (renderer.h) with the fly camera's pose. */

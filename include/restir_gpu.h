@@ -66,6 +66,8 @@ extern "C" {
 #define RESTIR_TRACE_CLOSEST_QUEUE 4     /* RESTIR_TRACE_CLOSEST through the persistent
                                             queue tracer (same results; no reference
                                             counterpart) */
+#define RESTIR_TRACE_ANY_WAVE 5          /* any hit in warp lock step (bvh.sh:177-212); rays
+                                            32i..32i+31 form one warp */
 
 /*
  * Everything the reference passes read from vec4 uniforms, by name. Values
@@ -141,7 +143,11 @@ typedef struct RestirParams
 	 * previousIndirect (restir.sh:265-298). */
 	float radiance_cache;
 	uint32_t cache_training_samples;  /* path suffixes traced per frame to train it */
-	float pad_params[2];
+	/* > 0.5: visibility rays walk the BVH in warp lock step (traceBvhWave,
+	 * bvh.sh:177-212, the reference's Vulkan build) instead of per lane
+	 * (traceBvhStackless); the hits are the same. */
+	float wave_visibility;
+	float pad_params[1];
 } RestirParams;
 
 /* Scene buffers, uploaded once per scene (renderer.cpp:365-419, 1170-1207). */

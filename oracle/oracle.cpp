@@ -122,6 +122,42 @@ extern "C" int oracle_trace(const RestirParams* params, const RestirScene* scene
 	Bvh base = makeBvh(scene);
 	const int threadCount = threads();
 	std::vector<Bvh> perThread(size_t(threadCount), base);
+	if (kind == RESTIR_TRACE_ANY_WAVE)
+	{
+		// Rays 32w .. 32w + 31 are the lanes of wave w.
+		const int64_t waves = (int64_t(n) + 31) / 32;
+		parallelFor(waves, 16, [&](int64_t wave, int thread)
+		{
+			Bvh& b = perThread[size_t(thread)];
+			const int64_t first = wave * 32;
+			const int count = int(std::min<int64_t>(32, int64_t(n) - first));
+			vec3 origin[32], direction[32];
+			float distance[32];
+			int hit[32];
+			for (int lane = 0; lane < count; ++lane)
+			{
+				const float* r = rays + 8 * (first + lane);
+				origin[lane] = vec3(r[0], r[1], r[2]);
+				direction[lane] = vec3(r[4], r[5], r[6]);
+				distance[lane] = r[3];
+				hit[lane] = -1;
+			}
+			if (b.available())
+			{
+				traceBvhWave(b, count, origin, direction, true, distance, hit);
+			}
+			for (int lane = 0; lane < count; ++lane)
+			{
+				hit_triangle[first + lane] = hit[lane];
+				hit_distance[first + lane] = distance[lane];
+			}
+		});
+		for (int t = 0; t < threadCount; ++t)
+		{
+			addCounts(perThread[size_t(t)], 0, 0);
+		}
+		return RESTIR_OK;
+	}
 	parallelFor(int64_t(n), 256, [&](int64_t i, int thread)
 	{
 		Bvh& b = perThread[size_t(thread)];

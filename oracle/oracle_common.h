@@ -260,6 +260,61 @@ inline int traceBvhStackless(const Bvh& b, vec3 _origin, vec3 _direction, bool _
 	return hit;
 }
 
+/* traceBvhWave (bvh.sh:177-212) for a wave of _count lanes: every step the
+ * wave takes the smallest node a lane still needs (WaveActiveMin), the lanes
+ * at that node test it; the step cap counts the wave's steps. */
+inline void traceBvhWave(const Bvh& b, int _count, const vec3* _origin, const vec3* _direction, bool _anyHit,
+	float* _distance, int* _hit)
+{
+	int node[32];
+	vec3 inverseDirection[32];
+	for (int lane = 0; lane < _count; ++lane)
+	{
+		inverseDirection[lane] = bvhInverseDirection(_direction[lane]);
+		node[lane] = 0;
+		_hit[lane] = -1;
+	}
+	int step = 0;
+	for (; step < kBvhMaxSteps; ++step)
+	{
+		int waveNode = b.nodeCount;
+		for (int lane = 0; lane < _count; ++lane)
+		{
+			waveNode = node[lane] < waveNode ? node[lane] : waveNode;
+		}
+		if (waveNode >= b.nodeCount)
+		{
+			break;
+		}
+		vec4 node0 = b.row(waveNode * 2);
+		vec4 node1 = b.row(waveNode * 2 + 1);
+		bool leaf = node1.w >= 0.0f;
+		for (int lane = 0; lane < _count; ++lane)
+		{
+			if (node[lane] != waveNode)
+			{
+				continue;
+			}
+			++b.nodeVisits;
+			if (intersectBox(_origin[lane], inverseDirection[lane], node0.xyz(), node1.xyz(), _distance[lane]) < 0.0f)
+			{
+				node[lane] = leaf ? node[lane] + 1 : int(-node1.w) - 1;
+				continue;
+			}
+			if (leaf)
+			{
+				_hit[lane] = bvhIntersectLeaf(b, _origin[lane], _direction[lane], int(node0.w), int(node1.w), _distance[lane],
+					_hit[lane]);
+			}
+			node[lane] = _anyHit && _hit[lane] >= 0 ? b.nodeCount : node[lane] + 1;
+		}
+	}
+	if (step == kBvhMaxSteps && b.status)
+	{
+		*b.status |= 1u;
+	}
+}
+
 inline int traceBvhSharedStack(const Bvh& b, vec3 _origin, vec3 _direction, float& _distance)
 {
 	vec3 inverseDirection = bvhInverseDirection(_direction);

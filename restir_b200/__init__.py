@@ -33,6 +33,7 @@ RAY_SCREEN, RAY_HYBRID, RAY_BVH = 0, 1, 2
 OK, ERROR_INVALID_ARGUMENT, ERROR_LAUNCH, ERROR_STEP_CAP, ERROR_UNSUPPORTED = 0, -1, -2, -3, -4
 ERROR_TIMEOUT, ERROR_OUT_OF_MEMORY, ERROR_TOO_LARGE = -5, -6, -7
 TRACE_CLOSEST, TRACE_ANY, TRACE_CLOSEST_STACKLESS, TRACE_CLOSEST_WATERTIGHT, TRACE_CLOSEST_QUEUE = 0, 1, 2, 3, 4
+TRACE_ANY_WAVE = 5
 PASS_NAMES = ["shadow", "gbuffer", "di_temporal", "di_spatial", "grid", "gi_temporal", "gi_spatial",
               "denoise", "composite", "reference", "cache"]
 

@@ -35,7 +35,8 @@ class RestirParams(C.Structure):
         ("shadows_enabled", C.c_float), ("shadow_face_size", C.c_uint32),
         ("sky_zenith", f4), ("sky_horizon", f4), ("sky_ground", f4),
         ("composite_options", f4),
-        ("radiance_cache", C.c_float), ("cache_training_samples", C.c_uint32), ("pad_params", C.c_float * 2),
+        ("radiance_cache", C.c_float), ("cache_training_samples", C.c_uint32), ("wave_visibility", C.c_float),
+        ("pad_params", C.c_float * 1),
     ]
 
 
@@ -103,6 +104,7 @@ class RestirSettings(C.Structure):
         ("trace_steps", C.c_int), ("di_candidates", C.c_int), ("di_spatial_taps", C.c_int),
         ("grid_table_size", C.c_uint32), ("grid_cell_capacity", C.c_uint32), ("grid_mode", C.c_uint32),
         ("wavefront", C.c_uint32), ("radiance_cache", C.c_uint32), ("cache_training_samples", C.c_uint32),
+        ("wave_visibility", C.c_uint32),
     ]
 
 

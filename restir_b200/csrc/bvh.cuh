@@ -160,6 +160,56 @@ __device__ inline int traceStacklessWalk(const BvhView& b, V3 o, V3 d, bool anyH
 	return hit;
 }
 
+// traceBvhWave (bvh.sh:177-212), the visibility rays of the reference's
+// Vulkan build: the lanes that call it walk the skip-link order in lock
+// step. Each step the warp takes the smallest node any lane still needs
+// (__reduce_min_sync; a finished lane asks for nodeCount), and the lanes at
+// that node test it while the others wait, so lanes on the same part of the
+// tree share every node fetch. A lane visits its nodes in the stackless
+// walk's order, so its hit is the stackless walk's; only the step cap counts
+// the warp's steps.
+__device__ inline int traceStacklessWave(const BvhView& b, V3 o, V3 d, bool anyHit, float& distance, TraceWork& work)
+{
+	const unsigned mask = __activemask();
+	V3 inv = bvhInverseDirection(d);
+	const int nodeCount = b.nodeCount;
+	int hit = -1;
+	int node = 0;
+	int step = 0;
+	for (; step < kBvhMaxSteps; ++step)
+	{
+		const int waveNode = int(__reduce_min_sync(mask, unsigned(node)));
+		if (waveNode >= nodeCount)
+		{
+			break;
+		}
+		if (node == waveNode)
+		{
+			++work.nodes;
+			V4 node0 = b.row(waveNode * 2);
+			V4 node1 = b.row(waveNode * 2 + 1);
+			bool leaf = node1.w >= 0.0f;
+			if (intersectBox(o, inv, node0.xyz(), node1.xyz(), distance) < 0.0f)
+			{
+				node = leaf ? node + 1 : int(-node1.w) - 1;
+			}
+			else
+			{
+				if (leaf)
+				{
+					hit = intersectLeaf(b, o, d, int(node0.w), int(node1.w), distance, hit, work);
+				}
+				node = anyHit && hit >= 0 ? nodeCount : node + 1;
+			}
+		}
+	}
+	if (step == kBvhMaxSteps)
+	{
+		raiseStatus(1u);
+	}
+	return hit;
+}
+
 // bvh.sh:216-295. stack: this thread's kBvhShortStack entries, stride apart
 // (shared memory, interleaved across the block's threads).
 __device__ inline int traceShortStack(const BvhView& b, V3 o, V3 d, float& distance, int* stack, int stride, TraceWork& work)
@@ -262,6 +312,25 @@ __device__ __forceinline__ int traceBvh(const BvhView& b, V3 o, V3 d, float maxD
 		kind = RESTIR_COUNT_ANY;
 	}
 	countWork(kind, work.nodes, work.triangles);
+	return hit;
+}
+
+// A visibility (any-hit) ray: traceBvh's stackless walk, or with wave set
+// the warp-lock-step walk of the reference's Vulkan build (same hits).
+__device__ __forceinline__ int traceVisibility(const BvhView& b, V3 o, V3 d, float maxDistance, float& distance, bool wave)
+{
+	if (!wave)
+	{
+		return traceBvh(b, o, d, maxDistance, true, distance, nullptr, 0);
+	}
+	distance = maxDistance;
+	if (!b.available())
+	{
+		return -1;
+	}
+	TraceWork work;
+	const int hit = traceStacklessWave(b, o, d, true, distance, work);
+	countWork(RESTIR_COUNT_ANY, work.nodes, work.triangles);
 	return hit;
 }
 

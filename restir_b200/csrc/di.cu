@@ -193,8 +193,8 @@ struct DiPass
 		V3 toPoint = point - origin;
 		float pointDistance = length(toPoint);
 		float occluderDistance = 0.0f;
-		return traceBvh(bvh, origin, toPoint / fmaxf(pointDistance, 0.0001f), pointDistance * 0.999f - kDiRayBias(), true,
-			occluderDistance, nullptr, 0) < 0;
+		return traceVisibility(bvh, origin, toPoint / fmaxf(pointDistance, 0.0001f), pointDistance * 0.999f - kDiRayBias(),
+			occluderDistance, P.wave_visibility > 0.5f) < 0;
 	}
 
 	__device__ __forceinline__ bool sameSurface(V3 p, V3 n, V3 otherP, V3 otherN, float radius) const

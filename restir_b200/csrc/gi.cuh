@@ -568,13 +568,15 @@ struct GiPass
 			visible = false;
 			if (bvh.available())
 			{
-				visible = traceBvh(bvh, origin, direction, kMaxBvhRayDistance(), true, occluderDistance, nullptr, 0) < 0;
+				visible = traceVisibility(bvh, origin, direction, kMaxBvhRayDistance(), occluderDistance,
+					P.wave_visibility > 0.5f) < 0;
 			}
 		}
 		else if (P.ray_mode == RESTIR_RAY_MODE_BVH && bvh.available())
 		{
 			float occluderDistance = 0.0f;
-			visible = traceBvh(bvh, origin, direction, sampleDistance - kRayBias(), true, occluderDistance, nullptr, 0) < 0;
+			visible = traceVisibility(bvh, origin, direction, sampleDistance - kRayBias(), occluderDistance,
+				P.wave_visibility > 0.5f) < 0;
 		}
 		else
 		{

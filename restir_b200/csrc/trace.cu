@@ -41,6 +41,10 @@ __global__ void __launch_bounds__(kTraceBlock) traceKernel(BvhView bvh, const fl
 	{
 		hit = traceBvh(bvh, o, d, a.w, false, distance, nullptr, 0);
 	}
+	else if (kind == RESTIR_TRACE_ANY_WAVE)
+	{
+		hit = traceVisibility(bvh, o, d, a.w, distance, true);
+	}
 	else
 	{
 		hit = traceWatertight(bvh, o, d, distance);
@@ -79,7 +83,7 @@ extern "C" int restir_trace(const RestirParams* params, const RestirScene* scene
 {
 	(void)params;
 	if (scene == nullptr || rays == nullptr || hit_triangle == nullptr || hit_distance == nullptr
-		|| kind < RESTIR_TRACE_CLOSEST || kind > RESTIR_TRACE_CLOSEST_QUEUE)
+		|| kind < RESTIR_TRACE_CLOSEST || kind > RESTIR_TRACE_ANY_WAVE)
 	{
 		return RESTIR_ERROR_INVALID_ARGUMENT;
 	}

@@ -84,6 +84,7 @@ extern "C" void restir_settings_default(RestirSettings* s)
 	s->wavefront = 1;
 	s->radiance_cache = 0;
 	s->cache_training_samples = 65536;
+	s->wave_visibility = 0;
 }
 
 extern "C" int restir_frame_params(const RestirSettings* requested, const RestirMeshDesc* scene, uint32_t light_count,
@@ -196,6 +197,7 @@ extern "C" int restir_frame_params(const RestirSettings* requested, const Restir
 	p->radiance_cache = (s.radiance_cache && s.wavefront && !state->reference_accumulating) ? 1.0f : 0.0f;
 	p->cache_training_samples = s.cache_training_samples < RESTIR_CACHE_MAX_BATCH ? s.cache_training_samples
 		: RESTIR_CACHE_MAX_BATCH;
+	p->wave_visibility = s.wave_visibility ? 1.0f : 0.0f;
 
 	// The shadow atlas (renderer.cpp:527-593): six faces of a slightly wider
 	// field of view than 90 degrees, a border of 4 texels.

@@ -69,6 +69,21 @@ def test_gi_temporal_wavefront_bit_exact(case):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("case", ["courtyard", "bvh-rays"])
+def test_wave_visibility_bit_exact(case):
+    """Visibility rays in warp lock step (traceBvhWave, the reference's Vulkan
+    path) reproduce the per-lane stackless walk's frame, pass by pass, as long
+    as no warp reaches the step cap (checked)."""
+    c, setup, settings = _case_setup(case)
+    settings.wave_visibility = 1
+    w, h = c["size"]
+    rb.status_flags()
+    report, _, _ = run_checked(setup, w, h, c["frames"], settings)
+    assert report == {}, report
+    assert rb.status_flags() & 1 == 0
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("case", ["cornell", "courtyard", "bvh-rays"])
 def test_gi_passes_with_radiance_cache_bit_exact(case):
     """With the radiance cache standing in for previousIndirect, the GI passes

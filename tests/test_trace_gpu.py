@@ -12,7 +12,7 @@ from tests.helpers import make_scene, seeded_rays
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
 KINDS = [rb.TRACE_CLOSEST, rb.TRACE_ANY, rb.TRACE_CLOSEST_STACKLESS, rb.TRACE_CLOSEST_WATERTIGHT,
-         rb.TRACE_CLOSEST_QUEUE]
+         rb.TRACE_CLOSEST_QUEUE, rb.TRACE_ANY_WAVE]
 
 
 def trace_both(setup, rays, kind, scene_host=None, scene_dev=None):
@@ -91,3 +91,20 @@ def test_empty_ray_set_and_invalid_arguments():
     assert lib.restir_trace(None, setup.device_scene(), d.data_ptr(), i.data_ptr(), d.data_ptr(), 0,
                             rb.TRACE_CLOSEST, None) == 0
     assert lib.restir_trace(None, setup.device_scene(), d.data_ptr(), i.data_ptr(), d.data_ptr(), 1, 9, None) == -1
+
+
+def test_oracle_wave_walk_matches_stackless_any_hit():
+    """The oracle's lock-step walk (bvh.sh:177-212) gives each lane the
+    stackless walk's any hit (bvh.sh:140-174): same triangles, same distances."""
+    setup = make_scene(rb.SCENE_COURTYARD, 0, 20000)
+    rays = seeded_rays(setup, 1 << 12, seed=14)
+    host = setup.host_scene()
+    out = {}
+    for kind in (rb.TRACE_ANY, rb.TRACE_ANY_WAVE):
+        ids = np.zeros(len(rays), np.int32)
+        t = np.zeros(len(rays), np.float32)
+        ob.load().oracle_trace(None, host, rays.ctypes.data, ids.ctypes.data, t.ctypes.data, len(rays), kind)
+        out[kind] = (ids, t)
+    np.testing.assert_array_equal(out[rb.TRACE_ANY_WAVE][0], out[rb.TRACE_ANY][0])
+    np.testing.assert_array_equal(out[rb.TRACE_ANY_WAVE][1].view(np.uint32), out[rb.TRACE_ANY][1].view(np.uint32))
+    assert (out[rb.TRACE_ANY][0] >= 0).mean() > 0.2
