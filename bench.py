@@ -247,6 +247,61 @@ def cache_kernels(args) -> None:
                       "status": rb.status_flags()}), flush=True)
 
 
+BATCH_SIZES = [(640, 360), (960, 540), (1280, 720), (1920, 1080), (800, 450), (1600, 900), (1024, 576), (1440, 810)]
+
+
+def batched(args) -> None:
+    """--batched: the batched form, 8 views of uneven resolution (640x360 to
+    1920x1080, each its own camera) of the 1M-triangle scene in one frame
+    (restir_batch_*: one scene, one shadow atlas, one GI ray queue and tracer
+    launch, one CUDA graph); the tracer shape from the autotuner. Beside it the
+    same views rendered one after another by one renderer."""
+    import torch
+    import restir_b200 as rb
+    mesh, settings = scene_and_settings(rb)
+    base = rb.frame_input(mesh, 64, 64)
+    inputs = [rb.frame_input(mesh, w, h, yaw=base.yaw + 0.3 * v, pitch=base.pitch)
+              for v, (w, h) in enumerate(BATCH_SIZES)]
+    batch = rb.Batch(settings, len(inputs))
+    batch.set_scene(mesh)
+    best = batch.autotune(inputs, frames=5)
+    for _ in range(args.warmup):
+        batch.render(inputs)
+    batch.synchronize()
+    stream = torch.cuda.ExternalStream(batch.stream)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(args.steps):
+        batch.render(inputs)
+    stop.record(stream)
+    torch.cuda.synchronize()
+    batch_ms = start.elapsed_time(stop) / args.steps
+    batch.close()
+    single = rb.Renderer(settings)
+    single.set_scene(mesh)
+    sequential = []
+    sstream = torch.cuda.ExternalStream(single.stream)
+    for frame in inputs:
+        for _ in range(args.warmup):
+            single.render(frame)
+        single.synchronize()
+        start.record(sstream)
+        for _ in range(args.steps):
+            single.render(frame)
+        stop.record(sstream)
+        torch.cuda.synchronize()
+        sequential.append(start.elapsed_time(stop) / args.steps)
+    single.close()
+    pixels = sum(w * h for w, h in BATCH_SIZES)
+    print(json.dumps({"batched": True, "views": [f"{w}x{h}" for w, h in BATCH_SIZES], "ms_per_batch_frame": batch_ms,
+                      "mpixels_per_s": pixels / (batch_ms * 1e-3) / 1e6, "sequential_ms": float(sum(sequential)),
+                      "sequential_per_view_ms": sequential, "speedup_vs_sequential": float(sum(sequential)) / batch_ms,
+                      "tuning": {"tracer_threads": best.tracer_threads,
+                                 "tracer_blocks_per_sm": best.tracer_blocks_per_sm,
+                                 "autotune_ms_per_frame": best.ms_per_frame},
+                      "status": rb.status_flags()}), flush=True)
+
+
 def max_over_ranks(values, dist, device: str) -> list:
     """Every rank's timings reduced to the maximum over the ranks (the job's
     time is its slowest replica's); every rank must call it. dist None: one
@@ -467,6 +522,8 @@ def main():
     parser.add_argument("--graph", action="store_true", help="replay each frame as a CUDA graph")
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--no-cache", action="store_true", help="skip the radiance-cache form's measurement")
+    parser.add_argument("--batched", action="store_true",
+                        help="the batched multi-view form (8 views of uneven resolution in one frame)")
     parser.add_argument("--cache-kernels", action="store_true",
                         help="time the radiance cache's query and training kernels alone (profiling)")
     parser.add_argument("--quick", action="store_true",
@@ -477,6 +534,8 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.gpus == 1 else 1)))
     if args.cache_kernels:
         cache_kernels(args)
+    elif args.batched:
+        batched(args)
     elif args.impl == "reference":
         reference_arm(args, rank, world)
     else:

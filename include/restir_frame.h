@@ -184,6 +184,41 @@ int restir_renderer_last_frame(void* renderer, RestirParams* params, RestirFrame
  * "gi.sample", "grid", "reference.mean", ...): pointer and byte size. */
 int restir_renderer_buffer(void* renderer, const char* name, void** pointer, uint64_t* bytes);
 
+/* --- Batches of views (no reference counterpart) ------------------------ */
+
+/* Several views of one scene (each with its own camera and resolution)
+ * rendered as one frame: the scene is uploaded once, the shadow atlas drawn
+ * once, the GI candidate rays of every view go to one ray queue that a single
+ * persistent tracer launch drains (restir_trace_queue), and the whole frame
+ * is one CUDA graph whose per-view branches run on their own streams. Each
+ * view's output equals a renderer's for that view alone. The radiance cache
+ * is not available in a batch (settings.radiance_cache is ignored). */
+typedef struct RestirBatchTuning
+{
+	uint32_t tracer_threads;       /* 64, 128 or 256 threads per block */
+	uint32_t tracer_blocks_per_sm; /* resident blocks per SM, 0: as many as fit */
+	float ms_per_frame;            /* autotune: the winner's device time per batch frame */
+} RestirBatchTuning;
+
+void* restir_batch_create(const RestirSettings* settings, uint32_t views);
+void restir_batch_destroy(void* batch);
+int restir_batch_set_scene(void* batch, void* mesh, int use_scene_defaults);
+int restir_batch_set_settings(void* batch, const RestirSettings* settings);
+/* inputs: one per view (width, height and camera of each). */
+int restir_batch_render(void* batch, const RestirFrameInput* inputs);
+/* Renders `frames` frames with each of a fixed list of tracer shapes and
+ * keeps the fastest (the frames advance the views' histories). */
+int restir_batch_autotune(void* batch, const RestirFrameInput* inputs, uint32_t frames, RestirBatchTuning* best);
+int restir_batch_set_tuning(void* batch, const RestirBatchTuning* tuning);
+int restir_batch_get_tuning(void* batch, RestirBatchTuning* tuning);
+int restir_batch_synchronize(void* batch);
+/* The stream the batch frame's graph is launched on. */
+void* restir_batch_stream(void* batch);
+/* A view's buffers and last frame, as restir_renderer_buffer / _last_frame. */
+int restir_batch_view_buffer(void* batch, uint32_t view, const char* name, void** pointer, uint64_t* bytes);
+int restir_batch_view_last_frame(void* batch, uint32_t view, RestirParams* params, RestirFramePlan* plan,
+	RestirFrameState* state);
+
 #ifdef __cplusplus
 }
 #endif

@@ -270,6 +270,33 @@ int restir_gi_temporal_wavefront(const RestirParams* params, const RestirScene* 
 	const uint16_t* surface_light, const RestirGiReservoirs* output, void* workspace, uint64_t workspace_bytes,
 	void* stream);
 
+/* No reference counterpart: the wavefront's three steps with a ray queue the
+ * caller owns, so that several views can fill one queue and have it traced
+ * by a single persistent launch (restir_batch_* does this):
+ *   restir_ray_queue_reset(queue)                         counters to zero
+ *   restir_gi_temporal_candidates(view ..., records, queue)   per view
+ *   restir_trace_queue(scene, queue, ...)                 once
+ *   restir_gi_temporal_shade(view ..., records, queue)        per view
+ * The outputs equal restir_gi_temporal's. queue: 256-byte aligned,
+ * restir_ray_queue_bytes(capacity) bytes, capacity >= the sum of the views'
+ * GI pixels x initial_candidates (rays past it are not traced: status bit
+ * 2). records: 256-byte aligned, restir_gi_candidate_records_bytes(params)
+ * per view. restir_trace_queue's threads (64, 128 or 256 per block) and
+ * blocks_per_sm (0: as many as fit) shape the resident grid. */
+uint64_t restir_ray_queue_bytes(uint32_t capacity);
+int restir_ray_queue_reset(void* queue, void* stream);
+uint64_t restir_gi_candidate_records_bytes(const RestirParams* params);
+int restir_gi_temporal_candidates(const RestirParams* params, const RestirScene* scene, const RestirGBuffer* gbuffer,
+	const RestirGiHistory* history, const uint32_t* previous_grid, const float* shadow_atlas,
+	const uint16_t* surface_light, void* records, uint64_t records_bytes, void* queue, uint32_t queue_capacity,
+	void* stream);
+int restir_trace_queue(const RestirScene* scene, void* queue, uint32_t queue_capacity, uint32_t threads,
+	uint32_t blocks_per_sm, void* stream);
+int restir_gi_temporal_shade(const RestirParams* params, const RestirScene* scene, const RestirGBuffer* gbuffer,
+	const RestirGiHistory* history, const uint32_t* previous_grid, const float* shadow_atlas,
+	const uint16_t* surface_light, const RestirGiReservoirs* output, const void* records, uint64_t records_bytes,
+	const void* queue, uint32_t queue_capacity, void* stream);
+
 /* color, moments: half4 at GI resolution. */
 int restir_gi_spatial(const RestirParams* params, const RestirScene* scene, const RestirGBuffer* gbuffer,
 	const RestirGiReservoirs* current, const uint32_t* current_grid, const RestirGiHistory* history,

@@ -109,6 +109,28 @@ _SIGNATURES = {
     "restir_renderer_last_frame": (C.c_int, [P, C.POINTER(RestirParams), C.POINTER(RestirFramePlan),
                                              C.POINTER(RestirFrameState)]),
     "restir_renderer_buffer": (C.c_int, [P, C.c_char_p, C.POINTER(P), C.POINTER(C.c_uint64)]),
+    "restir_batch_create": (P, [C.POINTER(RestirSettings), u32]),
+    "restir_batch_destroy": (None, [P]),
+    "restir_batch_set_scene": (C.c_int, [P, P, C.c_int]),
+    "restir_batch_set_settings": (C.c_int, [P, C.POINTER(RestirSettings)]),
+    "restir_batch_render": (C.c_int, [P, C.POINTER(RestirFrameInput)]),
+    "restir_batch_autotune": (C.c_int, [P, C.POINTER(RestirFrameInput), u32, C.POINTER(abi.RestirBatchTuning)]),
+    "restir_batch_set_tuning": (C.c_int, [P, C.POINTER(abi.RestirBatchTuning)]),
+    "restir_batch_get_tuning": (C.c_int, [P, C.POINTER(abi.RestirBatchTuning)]),
+    "restir_batch_synchronize": (C.c_int, [P]),
+    "restir_batch_stream": (P, [P]),
+    "restir_batch_view_buffer": (C.c_int, [P, u32, C.c_char_p, C.POINTER(P), C.POINTER(C.c_uint64)]),
+    "restir_batch_view_last_frame": (C.c_int, [P, u32, C.POINTER(RestirParams), C.POINTER(RestirFramePlan),
+                                               C.POINTER(RestirFrameState)]),
+    "restir_ray_queue_bytes": (C.c_uint64, [u32]),
+    "restir_ray_queue_reset": (C.c_int, [P, P]),
+    "restir_gi_candidate_records_bytes": (C.c_uint64, [C.POINTER(RestirParams)]),
+    "restir_gi_temporal_candidates": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirScene), C.POINTER(RestirGBuffer),
+                                                C.POINTER(RestirGiHistory), P, P, P, P, C.c_uint64, P, u32, P]),
+    "restir_trace_queue": (C.c_int, [C.POINTER(RestirScene), P, u32, u32, u32, P]),
+    "restir_gi_temporal_shade": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirScene), C.POINTER(RestirGBuffer),
+                                           C.POINTER(RestirGiHistory), P, P, P, C.POINTER(RestirGiReservoirs), P,
+                                           C.c_uint64, P, u32, P]),
     # restir_cache.h
     "restir_cache_config_default": (None, [C.POINTER(abi.RestirCacheConfig)]),
     "restir_cache_layout": (C.c_int, [C.POINTER(abi.RestirCacheConfig), C.POINTER(abi.RestirCacheLayout)]),
@@ -485,3 +507,79 @@ class RadianceCache:
     def scalars(self) -> abi.RestirCacheScalars:
         raw = self.state[self.layout.scalars:self.layout.scalars + C.sizeof(abi.RestirCacheScalars)].cpu().numpy()
         return abi.RestirCacheScalars.from_buffer_copy(raw.tobytes())
+
+
+class Batch:
+    """Several views of one scene rendered as one frame (include/restir_frame.h,
+    restir_batch_*): one scene upload, one shadow atlas, one GI ray queue
+    traced by a single persistent launch, one CUDA graph per frame."""
+
+    def __init__(self, settings: RestirSettings | None, views: int):
+        self._lib = load()
+        self.views = views
+        self.handle = self._lib.restir_batch_create(C.byref(settings) if settings is not None else None, views)
+        if not self.handle:
+            raise RuntimeError("restir_batch_create failed")
+
+    def set_scene(self, mesh: Mesh, use_scene_defaults: bool = True) -> None:
+        self.mesh = mesh
+        check(self._lib.restir_batch_set_scene(self.handle, mesh.handle, int(use_scene_defaults)), "batch set_scene")
+
+    def set_settings(self, settings: RestirSettings) -> None:
+        check(self._lib.restir_batch_set_settings(self.handle, C.byref(settings)), "batch set_settings")
+
+    @staticmethod
+    def _inputs(frame_inputs):
+        array = (RestirFrameInput * len(frame_inputs))(*frame_inputs)
+        return array
+
+    def render(self, frame_inputs) -> None:
+        check(self._lib.restir_batch_render(self.handle, self._inputs(frame_inputs)), "batch render")
+
+    def autotune(self, frame_inputs, frames: int = 5) -> abi.RestirBatchTuning:
+        best = abi.RestirBatchTuning()
+        check(self._lib.restir_batch_autotune(self.handle, self._inputs(frame_inputs), frames, C.byref(best)),
+              "batch autotune")
+        return best
+
+    @property
+    def tuning(self) -> abi.RestirBatchTuning:
+        t = abi.RestirBatchTuning()
+        check(self._lib.restir_batch_get_tuning(self.handle, C.byref(t)), "batch tuning")
+        return t
+
+    @tuning.setter
+    def tuning(self, t: abi.RestirBatchTuning) -> None:
+        check(self._lib.restir_batch_set_tuning(self.handle, C.byref(t)), "batch tuning")
+
+    @property
+    def stream(self) -> int:
+        return self._lib.restir_batch_stream(self.handle)
+
+    def synchronize(self) -> None:
+        check(self._lib.restir_batch_synchronize(self.handle), "batch synchronize")
+
+    def download(self, view: int, name: str, dtype) -> np.ndarray:
+        import torch
+        pointer, nbytes = C.c_void_p(), C.c_uint64()
+        check(self._lib.restir_batch_view_buffer(self.handle, view, name.encode(), C.byref(pointer), C.byref(nbytes)),
+              f"batch buffer {name}")
+        self.synchronize()
+        return device_view(pointer.value or 0, nbytes.value, torch.uint8).cpu().numpy().view(dtype)
+
+    def last_frame(self, view: int):
+        params, plan, state = RestirParams(), RestirFramePlan(), RestirFrameState()
+        check(self._lib.restir_batch_view_last_frame(self.handle, view, C.byref(params), C.byref(plan), C.byref(state)),
+              "batch last_frame")
+        return params, plan, state
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self._lib.restir_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

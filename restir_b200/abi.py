@@ -167,3 +167,7 @@ class RestirCacheScalars(C.Structure):
         ("loss", C.c_float), ("nonfinite", C.c_uint32), ("samples", C.c_uint32), ("blocks", C.c_uint32),
         ("beta1_power", C.c_float), ("beta2_power", C.c_float), ("pad", C.c_uint32 * 6),
     ]
+
+
+class RestirBatchTuning(C.Structure):
+    _fields_ = [("tracer_threads", C.c_uint32), ("tracer_blocks_per_sm", C.c_uint32), ("ms_per_frame", C.c_float)]

@@ -513,6 +513,14 @@ __global__ void __launch_bounds__(128) traceQueueKernel(BvhView bvh, RayQueue qu
 	traceQueueClosest<128>(bvh, queue, stackStorage);
 }
 
+// The queue tracer at other block sizes (restir_trace_queue's tuning knob).
+template<int kThreads>
+__global__ void __launch_bounds__(kThreads) traceQueueSizedKernel(BvhView bvh, RayQueue queue)
+{
+	__shared__ int stackStorage[kBvhShortStack * kThreads];
+	traceQueueClosest<kThreads>(bvh, queue, stackStorage);
+}
+
 __global__ void __launch_bounds__(kGiThreads, RESTIR_GI_TEMPORAL_MIN_BLOCKS) giTemporalShadeKernel(const RestirParams P,
 	BvhView bvh, GiBindings b, CandidateRecords records, RayQueue queue)
 {
@@ -826,6 +834,195 @@ extern "C" int restir_gi_temporal_wavefront(const RestirParams* params, const Re
 	giCandidatesKernel<<<blocks, kGiThreads, 0, s>>>(*params, bvh, b, w.records, w.queue);
 	traceQueueKernel<<<persistentBlocks(), 128, 0, s>>>(bvh, w.queue);
 	giTemporalShadeKernel<<<blocks, kGiThreads, 0, s>>>(*params, bvh, b, w.records, w.queue);
+	return launchStatus();
+}
+
+// --- the wavefront's three steps with a caller-owned, shareable ray queue ---------
+//
+// Several views (or frames) can append to one queue and have it traced by a
+// single persistent launch: restir_gi_temporal_candidates for each, one
+// restir_trace_queue, restir_gi_temporal_shade for each.
+
+namespace restir
+{
+namespace
+{
+
+// [2 counters][rays 32 B x c][hit triangles 4 B x c][hit distances 4 B x c], each on 256 bytes.
+RayQueue layoutQueue(void* base, uint32_t capacity, uint64_t* bytes)
+{
+	char* at = static_cast<char*>(base);
+	uint64_t offset = 0;
+	auto region = [&](uint64_t size) -> char*
+	{
+		char* start = at + offset;
+		offset += (size + 255u) & ~uint64_t(255u);
+		return start;
+	};
+	RayQueue q;
+	uint32_t* counters = reinterpret_cast<uint32_t*>(region(2 * sizeof(uint32_t)));
+	q.count = counters;
+	q.claimed = counters + 1;
+	q.rays = reinterpret_cast<float4*>(region(uint64_t(capacity) * 32));
+	q.hitTriangle = reinterpret_cast<int*>(region(uint64_t(capacity) * 4));
+	q.hitDistance = reinterpret_cast<float*>(region(uint64_t(capacity) * 4));
+	q.capacity = capacity;
+	if (bytes != nullptr)
+	{
+		*bytes = offset;
+	}
+	return q;
+}
+
+// [screen hits 16 B x n][slots 4 B x n], n = GI pixels x initial candidates.
+CandidateRecords layoutRecords(const RestirParams* p, void* base, uint64_t* bytes)
+{
+	const uint64_t n = uint64_t(p->gi_width) * p->gi_height * uint64_t(p->initial_candidates > 0 ? p->initial_candidates : 0);
+	CandidateRecords r;
+	r.screenHit = static_cast<float4*>(base);
+	r.slot = reinterpret_cast<int*>(static_cast<char*>(base) + ((n * 16 + 255u) & ~uint64_t(255u)));
+	r.candidates = p->initial_candidates;
+	if (bytes != nullptr)
+	{
+		*bytes = ((n * 16 + 255u) & ~uint64_t(255u)) + ((n * 4 + 255u) & ~uint64_t(255u));
+	}
+	return r;
+}
+
+bool aligned(const void* p)
+{
+	return p != nullptr && (reinterpret_cast<uintptr_t>(p) & 255u) == 0u;
+}
+
+template<int kThreads>
+int launchQueueTracer(const BvhView& bvh, const RayQueue& q, uint32_t blocksPerSm, cudaStream_t s)
+{
+	// SM count and resident blocks, queried once (not inside a stream capture on later calls).
+	static int sms = 0, fit = 0;
+	if (sms == 0)
+	{
+		int device = 0;
+		sms = 148;
+		if (cudaGetDevice(&device) == cudaSuccess)
+		{
+			cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+		}
+		if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, traceQueueSizedKernel<kThreads>, kThreads, 0) != cudaSuccess
+			|| fit < 1)
+		{
+			fit = 1;
+		}
+	}
+	int perSm = fit;
+	if (blocksPerSm > 0u && int(blocksPerSm) < perSm)
+	{
+		perSm = int(blocksPerSm);
+	}
+	traceQueueSizedKernel<kThreads><<<sms * perSm, kThreads, 0, s>>>(bvh, q);
+	return launchStatus();
+}
+
+} // namespace
+} // namespace restir
+
+extern "C" uint64_t restir_ray_queue_bytes(uint32_t capacity)
+{
+	uint64_t bytes = 0;
+	layoutQueue(nullptr, capacity, &bytes);
+	return bytes;
+}
+
+extern "C" int restir_ray_queue_reset(void* queue, void* stream)
+{
+	if (!aligned(queue))
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	return cudaMemsetAsync(queue, 0, 2 * sizeof(uint32_t), asStream(stream)) == cudaSuccess ? RESTIR_OK : RESTIR_ERROR_LAUNCH;
+}
+
+extern "C" uint64_t restir_gi_candidate_records_bytes(const RestirParams* params)
+{
+	if (params == nullptr)
+	{
+		return 0;
+	}
+	uint64_t bytes = 0;
+	layoutRecords(params, nullptr, &bytes);
+	return bytes;
+}
+
+extern "C" int restir_gi_temporal_candidates(const RestirParams* params, const RestirScene* scene, const RestirGBuffer* gbuffer,
+	const RestirGiHistory* history, const uint32_t* previous_grid, const float* shadow_atlas, const uint16_t* surface_light,
+	void* records, uint64_t records_bytes, void* queue, uint32_t queue_capacity, void* stream)
+{
+	if (!validCommon(params, scene, gbuffer, history, previous_grid, shadow_atlas) || params->initial_candidates < 0
+		|| !aligned(records) || !aligned(queue))
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	uint64_t needed = 0;
+	CandidateRecords r = layoutRecords(params, records, &needed);
+	if (records_bytes < needed)
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	const RayQueue q = layoutQueue(queue, queue_capacity, nullptr);
+	GiBindings b = bindings(gbuffer, history, previous_grid, shadow_atlas, surface_light);
+	const int groups = int((params->gi_width + 3) / 4 * ((params->gi_height + 7) / 8));
+	giCandidatesKernel<<<(groups + kGiWarps - 1) / kGiWarps, kGiThreads, 0, asStream(stream)>>>(*params, makeBvhView(scene), b,
+		r, q);
+	return launchStatus();
+}
+
+extern "C" int restir_trace_queue(const RestirScene* scene, void* queue, uint32_t queue_capacity, uint32_t threads,
+	uint32_t blocks_per_sm, void* stream)
+{
+	if (scene == nullptr || !aligned(queue))
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	const RayQueue q = layoutQueue(queue, queue_capacity, nullptr);
+	const BvhView bvh = makeBvhView(scene);
+	cudaStream_t s = asStream(stream);
+	switch (threads)
+	{
+	case 64:
+		return launchQueueTracer<64>(bvh, q, blocks_per_sm, s);
+	case 128:
+		return launchQueueTracer<128>(bvh, q, blocks_per_sm, s);
+	case 256:
+		return launchQueueTracer<256>(bvh, q, blocks_per_sm, s);
+	default:
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+}
+
+extern "C" int restir_gi_temporal_shade(const RestirParams* params, const RestirScene* scene, const RestirGBuffer* gbuffer,
+	const RestirGiHistory* history, const uint32_t* previous_grid, const float* shadow_atlas, const uint16_t* surface_light,
+	const RestirGiReservoirs* output, const void* records, uint64_t records_bytes, const void* queue,
+	uint32_t queue_capacity, void* stream)
+{
+	if (!validCommon(params, scene, gbuffer, history, previous_grid, shadow_atlas) || history->sample == nullptr
+		|| output == nullptr || output->sample == nullptr || output->receiver == nullptr || output->normal == nullptr
+		|| params->initial_candidates < 0 || !aligned(records) || !aligned(queue))
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	uint64_t needed = 0;
+	CandidateRecords r = layoutRecords(params, const_cast<void*>(records), &needed);
+	if (records_bytes < needed)
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	const RayQueue q = layoutQueue(const_cast<void*>(queue), queue_capacity, nullptr);
+	GiBindings b = bindings(gbuffer, history, previous_grid, shadow_atlas, surface_light);
+	b.outSample = reinterpret_cast<float4*>(output->sample);
+	b.outReceiver = reinterpret_cast<float4*>(output->receiver);
+	b.outNormal = reinterpret_cast<float4*>(output->normal);
+	const int groups = int((params->gi_width + 3) / 4 * ((params->gi_height + 7) / 8));
+	giTemporalShadeKernel<<<(groups + kGiWarps - 1) / kGiWarps, kGiThreads, 0, asStream(stream)>>>(*params, makeBvhView(scene),
+		b, r, q);
 	return launchStatus();
 }
 

@@ -16,6 +16,7 @@
 
 #include <cstring>
 #include <map>
+#include <memory>
 #include <new>
 #include <string>
 #include <vector>
@@ -37,8 +38,36 @@ struct Buffer
 	uint64_t bytes = 0;
 };
 
+// A scene's host data and device buffers (BVH, normals, materials, light
+// list, radiance cache), shared by every renderer drawing it.
+struct SceneState
+{
+	Mesh mesh;
+	BvhResult bvh;
+	LightListResult lights;
+	std::string lightsKey;
+	std::map<std::string, Buffer> buffers;
+	RestirCacheConfig cacheConfig = {};
+	bool has = false;
+
+	SceneState() = default;
+	SceneState(const SceneState&) = delete;
+	SceneState& operator=(const SceneState&) = delete;
+	~SceneState()
+	{
+		for (auto& kv : buffers)
+		{
+			cudaFree(kv.second.pointer);
+		}
+	}
+};
+
+class Batch;
+
 class Renderer
 {
+	friend class Batch;
+
 public:
 	explicit Renderer(const RestirSettings& settings) : m_settings(settings)
 	{
@@ -82,23 +111,23 @@ public:
 		cudaStreamSynchronize(m_stream);
 		releaseGraph();
 		releaseScene();
-		m_mesh = mesh;
+		m_scene->mesh = mesh;
 		if (useSceneDefaults)
 		{
 			std::memcpy(m_settings.light_position, mesh.lightPosition, sizeof(m_settings.light_position));
 			m_settings.sky_enabled = mesh.sky ? 1 : 0;
 		}
-		m_bvh = buildBvh(mesh, 8);
-		int status = upload(m_sceneBuffers["bvh"], m_bvh.data.data(), m_bvh.data.size() * sizeof(float));
-		status |= upload(m_sceneBuffers["normals"], m_bvh.triangleNormals.data(), m_bvh.triangleNormals.size() * sizeof(float));
-		status |= upload(m_sceneBuffers["materials"], mesh.materialData.data(), mesh.materialData.size() * sizeof(float));
-		m_lightsKey.clear();
+		m_scene->bvh = buildBvh(mesh, 8);
+		int status = upload(m_scene->buffers["bvh"], m_scene->bvh.data.data(), m_scene->bvh.data.size() * sizeof(float));
+		status |= upload(m_scene->buffers["normals"], m_scene->bvh.triangleNormals.data(), m_scene->bvh.triangleNormals.size() * sizeof(float));
+		status |= upload(m_scene->buffers["materials"], mesh.materialData.data(), mesh.materialData.size() * sizeof(float));
+		m_scene->lightsKey.clear();
 		status |= updateLights();
 		status |= initCache(mesh);
 		m_state.history_valid = 0;
 		m_state.di_valid = 0;
 		m_state.reference_frames = 0;
-		m_hasScene = status == 0;
+		m_scene->has = status == 0;
 		return status == 0 ? RESTIR_OK : RESTIR_ERROR_OUT_OF_MEMORY;
 	}
 
@@ -106,21 +135,21 @@ public:
 	// for every scene.
 	int initCache(const Mesh& mesh)
 	{
-		restir_cache_config_default(&m_cacheConfig);
+		restir_cache_config_default(&m_scene->cacheConfig);
 		for (int i = 0; i < 3; ++i)
 		{
-			m_cacheConfig.bounds_min[i] = mesh.boundsMin[i] - 0.01f * mesh.radius;
-			m_cacheConfig.bounds_max[i] = mesh.boundsMax[i] + 0.01f * mesh.radius;
+			m_scene->cacheConfig.bounds_min[i] = mesh.boundsMin[i] - 0.01f * mesh.radius;
+			m_scene->cacheConfig.bounds_max[i] = mesh.boundsMax[i] + 0.01f * mesh.radius;
 		}
-		const uint64_t bytes = restir_cache_state_bytes(&m_cacheConfig);
-		Buffer& b = m_sceneBuffers["cache.state"];
+		const uint64_t bytes = restir_cache_state_bytes(&m_scene->cacheConfig);
+		Buffer& b = m_scene->buffers["cache.state"];
 		b.bytes = bytes;
 		if (bytes == 0 || cudaMalloc(&b.pointer, bytes) != cudaSuccess)
 		{
 			b.pointer = nullptr;
 			return 1;
 		}
-		return restir_cache_init(&m_cacheConfig, b.pointer, m_stream) == RESTIR_OK ? 0 : 1;
+		return restir_cache_init(&m_scene->cacheConfig, b.pointer, m_stream) == RESTIR_OK ? 0 : 1;
 	}
 
 	int setSettings(const RestirSettings& settings)
@@ -131,9 +160,10 @@ public:
 
 	const RestirSettings& settings() const { return m_settings; }
 
-	int render(const RestirFrameInput& input, bool graph)
+	// The frame's uniforms, targets and workspace (the first part of render).
+	int prepare(const RestirFrameInput& input)
 	{
-		if (!m_hasScene)
+		if (!m_scene->has)
 		{
 			return RESTIR_ERROR_INVALID_ARGUMENT;
 		}
@@ -144,9 +174,9 @@ public:
 		}
 		RestirMeshDesc desc = describe();
 		RestirBvhDesc bvhDesc = {};
-		bvhDesc.node_count = m_bvh.nodeCount;
-		bvhDesc.triangle_offset = m_bvh.triangleOffset;
-		bvhDesc.triangle_count = m_bvh.triangleCount;
+		bvhDesc.node_count = m_scene->bvh.nodeCount;
+		bvhDesc.triangle_offset = m_scene->bvh.triangleOffset;
+		bvhDesc.triangle_count = m_scene->bvh.triangleCount;
 		// Reference mode: a moved camera starts the reference again (renderer.cpp:1050-1060).
 		if (m_state.reference_accumulating && m_state.reference_frames > 0
 			&& (std::memcmp(&m_referenceInput, &input, sizeof(input)) != 0))
@@ -154,7 +184,7 @@ public:
 			m_state.reference_frames = 0;
 		}
 		m_referenceInput = input;
-		status = restir_frame_params(&m_settings, &desc, m_lights.count, &bvhDesc, &input, &m_state, &m_params, &m_plan);
+		status = restir_frame_params(&m_settings, &desc, m_scene->lights.count, &bvhDesc, &input, &m_state, &m_params, &m_plan);
 		if (status != RESTIR_OK)
 		{
 			return status;
@@ -165,14 +195,30 @@ public:
 			status = ensureTargets(m_params);
 			if (status == RESTIR_OK)
 			{
-				status = restir_frame_params(&m_settings, &desc, m_lights.count, &bvhDesc, &input, &m_state, &m_params, &m_plan);
+				status = restir_frame_params(&m_settings, &desc, m_scene->lights.count, &bvhDesc, &input, &m_state, &m_params, &m_plan);
 			}
 			if (status != RESTIR_OK)
 			{
 				return status;
 			}
 		}
-		status = ensureWorkspace(m_params);
+		return ensureWorkspace(m_params);
+	}
+
+	// What the frame carries to the next: state and the ping-pong (the last part of render).
+	void advance(const RestirFrameInput& input)
+	{
+		restir_frame_advance(&m_params, &m_plan, &input, &m_state);
+		m_historyRead = 1 - m_historyRead;
+		if (m_plan.di_active)
+		{
+			m_diRead = 1 - m_diRead;
+		}
+	}
+
+	int render(const RestirFrameInput& input, bool graph)
+	{
+		int status = prepare(input);
 		if (status != RESTIR_OK)
 		{
 			return status;
@@ -193,14 +239,77 @@ public:
 		{
 			return status;
 		}
-		restir_frame_advance(&m_params, &m_plan, &input, &m_state);
-		m_historyRead = 1 - m_historyRead;
-		if (m_plan.di_active)
-		{
-			m_diRead = 1 - m_diRead;
-		}
+		advance(input);
 		m_timed = !graph;
 		return RESTIR_OK;
+	}
+
+	// --- batch views (restir_batch_*) ---
+
+	// Draws another renderer's scene (no copy; the scene lives while either holds it).
+	void shareScene(const Renderer& owner)
+	{
+		cudaStreamSynchronize(m_stream);
+		releaseGraph();
+		m_scene = owner.m_scene;
+		m_state.history_valid = 0;
+		m_state.di_valid = 0;
+		m_state.reference_frames = 0;
+	}
+
+	// The batch's shadow atlas and ray queue (null: the renderer's own).
+	void setBatch(float* atlas, void* queue, uint32_t capacity)
+	{
+		m_sharedAtlas = atlas;
+		m_batchQueue = queue;
+		m_batchQueueCapacity = capacity;
+	}
+
+	// The candidate records of this view's share of the batch's ray queue.
+	int ensureRecords()
+	{
+		const uint64_t needed = restir_gi_candidate_records_bytes(&m_params);
+		auto found = m_targets.find("gi.records");
+		if (found != m_targets.end() && found->second.bytes >= needed)
+		{
+			return RESTIR_OK;
+		}
+		cudaStreamSynchronize(m_stream);
+		if (found != m_targets.end())
+		{
+			cudaFree(found->second.pointer);
+			m_targets.erase(found);
+		}
+		Buffer b;
+		b.bytes = needed;
+		if (cudaMalloc(&b.pointer, needed) != cudaSuccess)
+		{
+			return RESTIR_ERROR_OUT_OF_MEMORY;
+		}
+		m_targets["gi.records"] = b;
+		return RESTIR_OK;
+	}
+
+	uint32_t candidateRays() const
+	{
+		return m_params.gi_width * m_params.gi_height * uint32_t(m_params.initial_candidates > 0 ? m_params.initial_candidates : 0);
+	}
+
+	const RestirParams& params() const { return m_params; }
+
+	RestirScene deviceScene()
+	{
+		RestirScene scene = {};
+		scene.bvh = static_cast<const float*>(m_scene->buffers["bvh"].pointer);
+		scene.node_count = m_scene->bvh.nodeCount;
+		scene.triangle_offset = m_scene->bvh.triangleOffset;
+		scene.triangle_count = m_scene->bvh.triangleCount;
+		scene.lights = static_cast<const float*>(m_scene->buffers["lights"].pointer);
+		scene.light_count = m_scene->lights.count;
+		scene.triangle_normals = static_cast<const float*>(m_scene->buffers["normals"].pointer);
+		scene.materials = static_cast<const float*>(m_scene->buffers["materials"].pointer);
+		scene.material_count = uint32_t(m_scene->mesh.materials.size());
+		return scene;
 	}
 
 	int measure(RestirMetrics* metrics)
@@ -322,8 +431,8 @@ public:
 		auto it = m_targets.find(name);
 		if (it == m_targets.end())
 		{
-			it = m_sceneBuffers.find(name);
-			if (it == m_sceneBuffers.end())
+			it = m_scene->buffers.find(name);
+			if (it == m_scene->buffers.end())
 			{
 				return RESTIR_ERROR_INVALID_ARGUMENT;
 			}
@@ -358,38 +467,38 @@ private:
 	RestirMeshDesc describe() const
 	{
 		RestirMeshDesc d = {};
-		d.triangle_count = m_mesh.triangleCount();
-		d.material_count = uint32_t(m_mesh.materials.size());
-		std::memcpy(d.bounds_min, m_mesh.boundsMin, sizeof(d.bounds_min));
-		std::memcpy(d.bounds_max, m_mesh.boundsMax, sizeof(d.bounds_max));
-		std::memcpy(d.center, m_mesh.center, sizeof(d.center));
-		d.radius = m_mesh.radius;
+		d.triangle_count = m_scene->mesh.triangleCount();
+		d.material_count = uint32_t(m_scene->mesh.materials.size());
+		std::memcpy(d.bounds_min, m_scene->mesh.boundsMin, sizeof(d.bounds_min));
+		std::memcpy(d.bounds_max, m_scene->mesh.boundsMax, sizeof(d.bounds_max));
+		std::memcpy(d.center, m_scene->mesh.center, sizeof(d.center));
+		d.radius = m_scene->mesh.radius;
 		return d;
 	}
 
 	// Renderer::updateLightList (renderer.cpp:1170-1207): rebuilt when its inputs change.
 	int updateLights()
 	{
-		if (!m_hasScene && m_bvh.nodeCount == 0)
+		if (!m_scene->has && m_scene->bvh.nodeCount == 0)
 		{
 			return RESTIR_OK;
 		}
-		const float scale = (m_mesh.radius / 1.75f) * (m_mesh.radius / 1.75f);
+		const float scale = (m_scene->mesh.radius / 1.75f) * (m_scene->mesh.radius / 1.75f);
 		std::string key = std::to_string(m_settings.emissive_lighting) + "/" + std::to_string(m_settings.extra_lights) + "/"
 			+ std::to_string(m_settings.extra_intensity) + "/" + std::to_string(m_settings.extra_seed) + "/" + std::to_string(scale);
-		if (key == m_lightsKey)
+		if (key == m_scene->lightsKey)
 		{
 			return RESTIR_OK;
 		}
-		m_lightsKey = key;
+		m_scene->lightsKey = key;
 		static const std::vector<Emitter> none;
-		m_lights = buildLightList(m_settings.emissive_lighting ? m_bvh.emitters : none, m_settings.extra_lights,
-			m_settings.extra_intensity, uint32_t(m_settings.extra_seed), m_mesh.boundsMin, m_mesh.boundsMax, scale);
+		m_scene->lights = buildLightList(m_settings.emissive_lighting ? m_scene->bvh.emitters : none, m_settings.extra_lights,
+			m_settings.extra_intensity, uint32_t(m_settings.extra_seed), m_scene->mesh.boundsMin, m_scene->mesh.boundsMax, scale);
 		cudaStreamSynchronize(m_stream);
-		Buffer& b = m_sceneBuffers["lights"];
+		Buffer& b = m_scene->buffers["lights"];
 		cudaFree(b.pointer);
 		b = Buffer();
-		std::vector<float> data = m_lights.data;
+		std::vector<float> data = m_scene->lights.data;
 		if (data.empty())
 		{
 			data.assign(16, 0.0f);
@@ -506,22 +615,27 @@ private:
 	}
 
 	// The passes of one frame, in the reference's order (renderer.cpp:527-1077).
-	int enqueue(bool events)
+	// part: the whole frame, or (for a batch of views sharing one ray queue)
+	// the passes up to the GI candidates, or the GI shading and the rest.
+	static constexpr int kWholeFrame = 0, kBeforeTrace = 1, kAfterTrace = 2;
+	int enqueue(bool events, int part = kWholeFrame)
 	{
+		const bool before = part != kAfterTrace;
+		const bool after = part != kBeforeTrace;
 		const RestirParams& P = m_params;
 		const RestirFramePlan& plan = m_plan;
 		const int hw = 1 - m_historyRead, hr = m_historyRead, dw = 1 - m_diRead, dr = m_diRead;
 		const std::string H = std::to_string(hw), R = std::to_string(hr);
 		RestirScene scene = {};
-		scene.bvh = static_cast<const float*>(m_sceneBuffers["bvh"].pointer);
-		scene.node_count = m_bvh.nodeCount;
-		scene.triangle_offset = m_bvh.triangleOffset;
-		scene.triangle_count = m_bvh.triangleCount;
-		scene.lights = static_cast<const float*>(m_sceneBuffers["lights"].pointer);
-		scene.light_count = m_lights.count;
-		scene.triangle_normals = static_cast<const float*>(m_sceneBuffers["normals"].pointer);
-		scene.materials = static_cast<const float*>(m_sceneBuffers["materials"].pointer);
-		scene.material_count = uint32_t(m_mesh.materials.size());
+		scene.bvh = static_cast<const float*>(m_scene->buffers["bvh"].pointer);
+		scene.node_count = m_scene->bvh.nodeCount;
+		scene.triangle_offset = m_scene->bvh.triangleOffset;
+		scene.triangle_count = m_scene->bvh.triangleCount;
+		scene.lights = static_cast<const float*>(m_scene->buffers["lights"].pointer);
+		scene.light_count = m_scene->lights.count;
+		scene.triangle_normals = static_cast<const float*>(m_scene->buffers["normals"].pointer);
+		scene.materials = static_cast<const float*>(m_scene->buffers["materials"].pointer);
+		scene.material_count = uint32_t(m_scene->mesh.materials.size());
 		RestirGBuffer gb = { p<uint8_t>("gbuffer.albedo"), p<uint8_t>("gbuffer.normal"), p<uint16_t>("gbuffer.emissive"),
 			p<uint8_t>("gbuffer.shading_normal"), p<float>("gbuffer.depth") };
 		void* s = m_stream;
@@ -547,12 +661,20 @@ private:
 				}
 			}
 		};
-		run(RESTIR_PASS_SHADOW, [&] { return restir_shadow_atlas(&P, &scene, p<float>("shadow.atlas"), s); });
-		run(RESTIR_PASS_GBUFFER, [&] { return restir_gbuffer_primary(&P, &scene, &gb, s); });
+		// A batch draws the shadow atlas once for all its views (it depends on the light and scene only).
+		float* atlas = m_sharedAtlas != nullptr ? m_sharedAtlas : p<float>("shadow.atlas");
+		if (before && m_sharedAtlas == nullptr)
+		{
+			run(RESTIR_PASS_SHADOW, [&] { return restir_shadow_atlas(&P, &scene, atlas, s); });
+		}
+		if (before)
+		{
+			run(RESTIR_PASS_GBUFFER, [&] { return restir_gbuffer_primary(&P, &scene, &gb, s); });
+		}
 		const std::string DW = std::to_string(dw), DR = std::to_string(dr);
 		RestirDiReservoirs diPrevious = { p<float>("di.sample" + DR), p<float>("di.receiver" + DR), p<uint16_t>("di.normal" + DR) };
 		RestirDiReservoirs diCurrent = { p<float>("di.sample" + DW), p<float>("di.receiver" + DW), p<uint16_t>("di.normal" + DW) };
-		if (plan.di_active)
+		if (before && plan.di_active)
 		{
 			run(RESTIR_PASS_DI_TEMPORAL, [&] { return restir_di_temporal(&P, &scene, &gb, &diPrevious, &diCurrent, s); });
 			run(RESTIR_PASS_DI_SPATIAL, [&] {
@@ -562,37 +684,56 @@ private:
 		const uint16_t* surface = plan.surface_light_is_di ? (plan.di_active ? p<uint16_t>("di.diffuse") : p<uint16_t>("black"))
 			: p<uint16_t>("gbuffer.emissive");
 		uint32_t* gridWrite = p<uint32_t>("grid" + H);
-		run(RESTIR_PASS_GRID, [&] {
-			return restir_grid_clear(&P, gridWrite, s) | restir_grid_insert(&P, &gb, gridWrite, s);
-		});
+		if (before)
+		{
+			run(RESTIR_PASS_GRID, [&] {
+				return restir_grid_clear(&P, gridWrite, s) | restir_grid_insert(&P, &gb, gridWrite, s);
+			});
+		}
 		RestirGiHistory history = { p<float>("gi.sample" + R), p<float>("gi.receiver" + R), p<float>("gi.normal" + R),
 			plan.denoiser ? p<uint16_t>("filtered" + R) : p<uint16_t>("gi.color" + R), p<uint16_t>("gi.moments" + R) };
 		RestirGiReservoirs current = { p<float>("gi.sample" + H), p<float>("gi.receiver" + H), p<float>("gi.normal" + H) };
 		const bool cached = P.radiance_cache > 0.5f;
-		void* cacheState = m_sceneBuffers["cache.state"].pointer;
-		run(RESTIR_PASS_GI_TEMPORAL, [&] {
+		void* cacheState = m_scene->buffers["cache.state"].pointer;
+		if (part != kWholeFrame)
+		{
+			// The batch's shared ray queue: candidates before its one tracer launch, shading after.
+			const Buffer& r = m_targets["gi.records"];
+			run(RESTIR_PASS_GI_TEMPORAL, [&] {
+				return part == kBeforeTrace
+					? restir_gi_temporal_candidates(&P, &scene, &gb, &history, p<uint32_t>("grid" + R), atlas, surface, r.pointer,
+						r.bytes, m_batchQueue, m_batchQueueCapacity, s)
+					: restir_gi_temporal_shade(&P, &scene, &gb, &history, p<uint32_t>("grid" + R), atlas, surface, &current,
+						r.pointer, r.bytes, m_batchQueue, m_batchQueueCapacity, s);
+			});
+		}
+		else run(RESTIR_PASS_GI_TEMPORAL, [&] {
 			const Buffer& w = m_targets["gi.workspace"];
 			if (cached)
 			{
-				return restir_gi_temporal_cached(&P, &scene, &gb, &history, p<uint32_t>("grid" + R), p<float>("shadow.atlas"),
-					surface, &current, &m_cacheConfig, cacheState, w.pointer, w.bytes, s);
+				return restir_gi_temporal_cached(&P, &scene, &gb, &history, p<uint32_t>("grid" + R), atlas,
+					surface, &current, &m_scene->cacheConfig, cacheState, w.pointer, w.bytes, s);
 			}
 			if (m_settings.wavefront)
 			{
-				return restir_gi_temporal_wavefront(&P, &scene, &gb, &history, p<uint32_t>("grid" + R), p<float>("shadow.atlas"),
+				return restir_gi_temporal_wavefront(&P, &scene, &gb, &history, p<uint32_t>("grid" + R), atlas,
 					surface, &current, w.pointer, w.bytes, s);
 			}
-			return restir_gi_temporal(&P, &scene, &gb, &history, p<uint32_t>("grid" + R), p<float>("shadow.atlas"), surface,
+			return restir_gi_temporal(&P, &scene, &gb, &history, p<uint32_t>("grid" + R), atlas, surface,
 				&current, s);
 		});
+		if (!after)
+		{
+			return status == RESTIR_OK ? RESTIR_OK : RESTIR_ERROR_LAUNCH;
+		}
 		run(RESTIR_PASS_GI_SPATIAL, [&] {
 			if (cached)
 			{
 				const Buffer& w = m_targets["gi.workspace"];
-				return restir_gi_spatial_cached(&P, &scene, &gb, &current, gridWrite, &history, p<float>("shadow.atlas"), surface,
-					p<uint16_t>("gi.color" + H), p<uint16_t>("gi.moments" + H), &m_cacheConfig, cacheState, w.pointer, w.bytes, s);
+				return restir_gi_spatial_cached(&P, &scene, &gb, &current, gridWrite, &history, atlas, surface,
+					p<uint16_t>("gi.color" + H), p<uint16_t>("gi.moments" + H), &m_scene->cacheConfig, cacheState, w.pointer, w.bytes, s);
 			}
-			return restir_gi_spatial(&P, &scene, &gb, &current, gridWrite, &history, p<float>("shadow.atlas"), surface,
+			return restir_gi_spatial(&P, &scene, &gb, &current, gridWrite, &history, atlas, surface,
 				p<uint16_t>("gi.color" + H), p<uint16_t>("gi.moments" + H), s);
 		});
 		if (cached)
@@ -600,7 +741,7 @@ private:
 			// Training after the frame's queries: every query of a frame sees the same weights.
 			run(RESTIR_PASS_CACHE, [&] {
 				const Buffer& w = m_targets["gi.workspace"];
-				return restir_cache_train_frame(&P, &scene, &gb, p<float>("shadow.atlas"), &m_cacheConfig, cacheState, w.pointer,
+				return restir_cache_train_frame(&P, &scene, &gb, atlas, &m_scene->cacheConfig, cacheState, w.pointer,
 					w.bytes, s);
 			});
 		}
@@ -624,7 +765,7 @@ private:
 		const uint16_t* diDiffuse = plan.di_active ? p<uint16_t>("di.diffuse") : p<uint16_t>("black");
 		const uint16_t* diSpecular = plan.di_active ? p<uint16_t>("di.specular") : p<uint16_t>("black");
 		run(RESTIR_PASS_COMPOSITE, [&] {
-			return restir_composite(&P, &gb, p<float>("shadow.atlas"), p<uint16_t>(denoised), diDiffuse, diSpecular,
+			return restir_composite(&P, &gb, atlas, p<uint16_t>(denoised), diDiffuse, diSpecular,
 				p<uint16_t>("hdr"), s);
 		});
 		if (plan.reference_accumulate)
@@ -693,14 +834,10 @@ private:
 		m_targets.clear();
 	}
 
+	// A fresh, empty scene; the previous one is freed when no renderer holds it.
 	void releaseScene()
 	{
-		for (auto& kv : m_sceneBuffers)
-		{
-			cudaFree(kv.second.pointer);
-		}
-		m_sceneBuffers.clear();
-		m_hasScene = false;
+		m_scene = std::make_shared<SceneState>();
 	}
 
 	RestirSettings m_settings;
@@ -708,22 +845,20 @@ private:
 	RestirParams m_params = {};
 	RestirFramePlan m_plan = {};
 	RestirFrameInput m_referenceInput = {};
-	Mesh m_mesh;
-	BvhResult m_bvh;
-	LightListResult m_lights;
-	std::string m_lightsKey;
-	std::map<std::string, Buffer> m_sceneBuffers;
+	std::shared_ptr<SceneState> m_scene = std::make_shared<SceneState>();
+	// Set by a batch: the shared shadow atlas and ray queue.
+	float* m_sharedAtlas = nullptr;
+	void* m_batchQueue = nullptr;
+	uint32_t m_batchQueueCapacity = 0;
 	std::map<std::string, Buffer> m_targets;
 	uint32_t m_width = 0, m_height = 0, m_giWidth = 0, m_giHeight = 0, m_faceSize = 0, m_tableSize = 0, m_capacity = 0;
 	int m_historyRead = 0;
 	int m_diRead = 0;
-	bool m_hasScene = false;
 	bool m_timed = false;
 	// Per-pass events of the last kEventRing stream-launched frames.
 	static constexpr uint32_t kEventRing = 128;
 	bool m_passRan[kEventRing][RESTIR_PASS_COUNT] = {};
 	cudaEvent_t m_events[kEventRing][RESTIR_PASS_COUNT][2] = {};  // start, end of each pass
-	RestirCacheConfig m_cacheConfig = {};
 	uint32_t m_slot = 0;
 	uint32_t m_lastSlot = 0;
 	uint32_t m_timedFrames = 0;
@@ -733,9 +868,336 @@ private:
 	uint64_t* m_profile = nullptr;
 };
 
+// Several views of one scene rendered as one frame (no reference
+// counterpart): the views share the scene's buffers, one shadow atlas (it
+// depends on the light and the scene only) and one GI ray queue that a single
+// persistent tracer launch drains; the frame is captured as one CUDA graph in
+// which each view's passes run on its own stream, so that small views fill
+// the GPU together. Every view's output equals what a Renderer of that view
+// alone produces.
+class Batch
+{
+public:
+	Batch(const RestirSettings& settings, uint32_t views)
+	{
+		RestirSettings s = settings;
+		s.radiance_cache = 0;  // the batch path runs the plain GI passes
+		s.wavefront = 1;
+		for (uint32_t v = 0; v < views; ++v)
+		{
+			m_views.push_back(new (std::nothrow) Renderer(s));
+		}
+		cudaStreamCreateWithFlags(&m_stream, cudaStreamNonBlocking);
+		cudaEventCreateWithFlags(&m_fork, cudaEventDisableTiming);
+		cudaEventCreateWithFlags(&m_traced, cudaEventDisableTiming);
+		m_joins.resize(2 * views);
+		for (cudaEvent_t& e : m_joins)
+		{
+			cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+		}
+		m_tuning.tracer_threads = 128;
+		m_tuning.tracer_blocks_per_sm = 0;
+		m_tuning.ms_per_frame = 0.0f;
+	}
+
+	~Batch()
+	{
+		synchronize();
+		if (m_graphExec != nullptr)
+		{
+			cudaGraphExecDestroy(m_graphExec);
+		}
+		for (Renderer* r : m_views)
+		{
+			delete r;
+		}
+		cudaFree(m_queue);
+		cudaFree(m_atlas);
+		for (cudaEvent_t e : m_joins)
+		{
+			cudaEventDestroy(e);
+		}
+		cudaEventDestroy(m_fork);
+		cudaEventDestroy(m_traced);
+		cudaStreamDestroy(m_stream);
+	}
+
+	bool valid() const
+	{
+		for (Renderer* r : m_views)
+		{
+			if (r == nullptr)
+			{
+				return false;
+			}
+		}
+		return !m_views.empty() && m_stream != nullptr;
+	}
+
+	uint32_t views() const { return uint32_t(m_views.size()); }
+	Renderer& view(uint32_t v) { return *m_views[v]; }
+	cudaStream_t stream() const { return m_stream; }
+	const RestirBatchTuning& tuning() const { return m_tuning; }
+
+	int setTuning(const RestirBatchTuning& t)
+	{
+		if (t.tracer_threads != 64 && t.tracer_threads != 128 && t.tracer_threads != 256)
+		{
+			return RESTIR_ERROR_INVALID_ARGUMENT;
+		}
+		m_tuning.tracer_threads = t.tracer_threads;
+		m_tuning.tracer_blocks_per_sm = t.tracer_blocks_per_sm;
+		return RESTIR_OK;
+	}
+
+	int setScene(const Mesh& mesh, bool useSceneDefaults)
+	{
+		synchronize();
+		int status = m_views[0]->setScene(mesh, useSceneDefaults);
+		for (uint32_t v = 1; v < views() && status == RESTIR_OK; ++v)
+		{
+			status = m_views[v]->setSettings(m_views[0]->settings());
+			m_views[v]->shareScene(*m_views[0]);
+		}
+		return status;
+	}
+
+	int setSettings(const RestirSettings& settings)
+	{
+		RestirSettings s = settings;
+		s.radiance_cache = 0;
+		s.wavefront = 1;
+		int status = RESTIR_OK;
+		for (Renderer* r : m_views)
+		{
+			status |= r->setSettings(s);
+		}
+		return status == RESTIR_OK ? RESTIR_OK : RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+
+	int render(const RestirFrameInput* inputs)
+	{
+		uint32_t rays = 0;
+		for (uint32_t v = 0; v < views(); ++v)
+		{
+			int status = m_views[v]->prepare(inputs[v]);
+			if (status == RESTIR_OK)
+			{
+				status = m_views[v]->ensureRecords();
+			}
+			if (status != RESTIR_OK)
+			{
+				return status;
+			}
+			rays += m_views[v]->candidateRays();
+		}
+		const RestirParams& first = m_views[0]->params();
+		int status = ensureShared(rays, 6ull * first.shadow_face_size * first.shadow_face_size * 4);
+		if (status != RESTIR_OK)
+		{
+			return status;
+		}
+		for (Renderer* r : m_views)
+		{
+			r->setBatch(m_atlas, m_queue, m_queueCapacity);
+		}
+		status = launchFrame();
+		if (status != RESTIR_OK)
+		{
+			return status;
+		}
+		for (uint32_t v = 0; v < views(); ++v)
+		{
+			m_views[v]->advance(inputs[v]);
+		}
+		return RESTIR_OK;
+	}
+
+	// Tries tracer shapes (threads per block x resident blocks per SM) on
+	// `frames` frames each and keeps the fastest (device time of the whole
+	// batch frame, CUDA events on the batch stream).
+	int autotune(const RestirFrameInput* inputs, uint32_t frames, RestirBatchTuning* best)
+	{
+		static const uint32_t shapes[][2] = { { 128, 0 }, { 64, 0 }, { 256, 0 }, { 128, 4 }, { 128, 2 }, { 256, 2 } };
+		cudaEvent_t start, stop;
+		cudaEventCreate(&start);
+		cudaEventCreate(&stop);
+		RestirBatchTuning winner = m_tuning;
+		winner.ms_per_frame = 0.0f;
+		int status = RESTIR_OK;
+		for (const auto& shape : shapes)
+		{
+			m_tuning.tracer_threads = shape[0];
+			m_tuning.tracer_blocks_per_sm = shape[1];
+			status = render(inputs);  // warm: capture, instantiate
+			cudaEventRecord(start, m_stream);
+			for (uint32_t f = 0; f < frames && status == RESTIR_OK; ++f)
+			{
+				status = render(inputs);
+			}
+			cudaEventRecord(stop, m_stream);
+			if (status != RESTIR_OK || cudaEventSynchronize(stop) != cudaSuccess)
+			{
+				status = status != RESTIR_OK ? status : RESTIR_ERROR_LAUNCH;
+				break;
+			}
+			float ms = 0.0f;
+			cudaEventElapsedTime(&ms, start, stop);
+			ms /= float(frames > 0 ? frames : 1);
+			if (winner.ms_per_frame == 0.0f || ms < winner.ms_per_frame)
+			{
+				winner.tracer_threads = shape[0];
+				winner.tracer_blocks_per_sm = shape[1];
+				winner.ms_per_frame = ms;
+			}
+		}
+		cudaEventDestroy(start);
+		cudaEventDestroy(stop);
+		m_tuning = winner;
+		if (best != nullptr)
+		{
+			*best = winner;
+		}
+		return status;
+	}
+
+	int synchronize()
+	{
+		int status = cudaStreamSynchronize(m_stream) == cudaSuccess ? RESTIR_OK : RESTIR_ERROR_LAUNCH;
+		for (Renderer* r : m_views)
+		{
+			if (r != nullptr && cudaStreamSynchronize(r->stream()) != cudaSuccess)
+			{
+				status = RESTIR_ERROR_LAUNCH;
+			}
+		}
+		return status;
+	}
+
+private:
+	int ensureShared(uint32_t rays, uint64_t atlasBytes)
+	{
+		if (rays > m_queueCapacity || m_queue == nullptr)
+		{
+			synchronize();
+			releaseGraph();
+			cudaFree(m_queue);
+			m_queue = nullptr;
+			if (cudaMalloc(&m_queue, restir_ray_queue_bytes(rays)) != cudaSuccess)
+			{
+				m_queueCapacity = 0;
+				m_queue = nullptr;
+				return RESTIR_ERROR_OUT_OF_MEMORY;
+			}
+			m_queueCapacity = rays;
+		}
+		if (atlasBytes > m_atlasBytes || m_atlas == nullptr)
+		{
+			synchronize();
+			releaseGraph();
+			cudaFree(m_atlas);
+			m_atlas = nullptr;
+			if (cudaMalloc(reinterpret_cast<void**>(&m_atlas), atlasBytes) != cudaSuccess)
+			{
+				m_atlasBytes = 0;
+				return RESTIR_ERROR_OUT_OF_MEMORY;
+			}
+			m_atlasBytes = atlasBytes;
+		}
+		return RESTIR_OK;
+	}
+
+	// The frame as one graph: queue reset and the shared atlas, then every
+	// view's passes up to its GI candidates on its own stream, the one tracer
+	// launch, every view's GI shading and later passes.
+	int launchFrame()
+	{
+		RestirScene scene = m_views[0]->deviceScene();
+		const RestirParams& first = m_views[0]->params();
+		cudaGraph_t graph = nullptr;
+		if (cudaStreamBeginCapture(m_stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+		{
+			return RESTIR_ERROR_LAUNCH;
+		}
+		int status = restir_ray_queue_reset(m_queue, m_stream);
+		status |= restir_shadow_atlas(&first, &scene, m_atlas, m_stream);
+		cudaEventRecord(m_fork, m_stream);
+		for (uint32_t v = 0; v < views(); ++v)
+		{
+			cudaStream_t s = m_views[v]->stream();
+			cudaStreamWaitEvent(s, m_fork, 0);
+			status |= m_views[v]->enqueue(false, Renderer::kBeforeTrace);
+			cudaEventRecord(m_joins[2 * v], s);
+			cudaStreamWaitEvent(m_stream, m_joins[2 * v], 0);
+		}
+		status |= restir_trace_queue(&scene, m_queue, m_queueCapacity, m_tuning.tracer_threads, m_tuning.tracer_blocks_per_sm,
+			m_stream);
+		cudaEventRecord(m_traced, m_stream);
+		for (uint32_t v = 0; v < views(); ++v)
+		{
+			cudaStream_t s = m_views[v]->stream();
+			cudaStreamWaitEvent(s, m_traced, 0);
+			status |= m_views[v]->enqueue(false, Renderer::kAfterTrace);
+			cudaEventRecord(m_joins[2 * v + 1], s);
+			cudaStreamWaitEvent(m_stream, m_joins[2 * v + 1], 0);
+		}
+		if (cudaStreamEndCapture(m_stream, &graph) != cudaSuccess || status != RESTIR_OK)
+		{
+			if (graph != nullptr)
+			{
+				cudaGraphDestroy(graph);
+			}
+			cudaGetLastError();
+			return RESTIR_ERROR_LAUNCH;
+		}
+		bool updated = false;
+		if (m_graphExec != nullptr)
+		{
+			cudaGraphExecUpdateResultInfo info;
+			updated = cudaGraphExecUpdate(m_graphExec, graph, &info) == cudaSuccess;
+			if (!updated)
+			{
+				cudaGetLastError();
+				cudaGraphExecDestroy(m_graphExec);
+				m_graphExec = nullptr;
+			}
+		}
+		if (!updated && cudaGraphInstantiate(&m_graphExec, graph, 0) != cudaSuccess)
+		{
+			cudaGraphDestroy(graph);
+			m_graphExec = nullptr;
+			return RESTIR_ERROR_LAUNCH;
+		}
+		cudaGraphDestroy(graph);
+		return cudaGraphLaunch(m_graphExec, m_stream) == cudaSuccess ? RESTIR_OK : RESTIR_ERROR_LAUNCH;
+	}
+
+	void releaseGraph()
+	{
+		if (m_graphExec != nullptr)
+		{
+			cudaGraphExecDestroy(m_graphExec);
+			m_graphExec = nullptr;
+		}
+	}
+
+	std::vector<Renderer*> m_views;
+	cudaStream_t m_stream = nullptr;
+	cudaEvent_t m_fork = nullptr;
+	cudaEvent_t m_traced = nullptr;
+	std::vector<cudaEvent_t> m_joins;
+	cudaGraphExec_t m_graphExec = nullptr;
+	void* m_queue = nullptr;
+	uint32_t m_queueCapacity = 0;
+	float* m_atlas = nullptr;
+	uint64_t m_atlasBytes = 0;
+	RestirBatchTuning m_tuning = {};
+};
+
 } // namespace
 } // namespace restir
 
+using restir::Batch;
 using restir::Renderer;
 
 extern "C" void* restir_renderer_create(const RestirSettings* settings)
@@ -877,4 +1339,121 @@ extern "C" int restir_renderer_buffer(void* renderer, const char* name, void** p
 		return RESTIR_ERROR_INVALID_ARGUMENT;
 	}
 	return static_cast<Renderer*>(renderer)->buffer(name, pointer, bytes);
+}
+
+// --- batches --------------------------------------------------------------------
+
+extern "C" void* restir_batch_create(const RestirSettings* settings, uint32_t views)
+{
+	if (views == 0u || views > 64u)
+	{
+		return nullptr;
+	}
+	RestirSettings s;
+	if (settings != nullptr)
+	{
+		s = *settings;
+	}
+	else
+	{
+		restir_settings_default(&s);
+	}
+	Batch* batch = new (std::nothrow) Batch(s, views);
+	if (batch != nullptr && !batch->valid())
+	{
+		delete batch;
+		return nullptr;
+	}
+	return batch;
+}
+
+extern "C" void restir_batch_destroy(void* batch)
+{
+	delete static_cast<Batch*>(batch);
+}
+
+extern "C" int restir_batch_set_scene(void* batch, void* mesh, int use_scene_defaults)
+{
+	if (batch == nullptr || mesh == nullptr)
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	return static_cast<Batch*>(batch)->setScene(*static_cast<restir::Mesh*>(mesh), use_scene_defaults != 0);
+}
+
+extern "C" int restir_batch_set_settings(void* batch, const RestirSettings* settings)
+{
+	if (batch == nullptr || settings == nullptr)
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	return static_cast<Batch*>(batch)->setSettings(*settings);
+}
+
+extern "C" int restir_batch_render(void* batch, const RestirFrameInput* inputs)
+{
+	if (batch == nullptr || inputs == nullptr)
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	return static_cast<Batch*>(batch)->render(inputs);
+}
+
+extern "C" int restir_batch_autotune(void* batch, const RestirFrameInput* inputs, uint32_t frames, RestirBatchTuning* best)
+{
+	if (batch == nullptr || inputs == nullptr)
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	return static_cast<Batch*>(batch)->autotune(inputs, frames, best);
+}
+
+extern "C" int restir_batch_set_tuning(void* batch, const RestirBatchTuning* tuning)
+{
+	if (batch == nullptr || tuning == nullptr)
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	return static_cast<Batch*>(batch)->setTuning(*tuning);
+}
+
+extern "C" int restir_batch_get_tuning(void* batch, RestirBatchTuning* tuning)
+{
+	if (batch == nullptr || tuning == nullptr)
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	*tuning = static_cast<Batch*>(batch)->tuning();
+	return RESTIR_OK;
+}
+
+extern "C" int restir_batch_synchronize(void* batch)
+{
+	return batch != nullptr ? static_cast<Batch*>(batch)->synchronize() : RESTIR_ERROR_INVALID_ARGUMENT;
+}
+
+extern "C" void* restir_batch_stream(void* batch)
+{
+	return batch != nullptr ? static_cast<void*>(static_cast<Batch*>(batch)->stream()) : nullptr;
+}
+
+extern "C" int restir_batch_view_buffer(void* batch, uint32_t view, const char* name, void** pointer, uint64_t* bytes)
+{
+	if (batch == nullptr || view >= static_cast<Batch*>(batch)->views() || name == nullptr || pointer == nullptr
+		|| bytes == nullptr)
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	return static_cast<Batch*>(batch)->view(view).buffer(name, pointer, bytes);
+}
+
+extern "C" int restir_batch_view_last_frame(void* batch, uint32_t view, RestirParams* params, RestirFramePlan* plan,
+	RestirFrameState* state)
+{
+	if (batch == nullptr || view >= static_cast<Batch*>(batch)->views())
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	static_cast<Batch*>(batch)->view(view).lastFrame(params, plan, state);
+	return RESTIR_OK;
 }
