@@ -366,7 +366,12 @@ __device__ inline int traceNearestFirst(const BvhView& b, V3 o, V3 d, float& dis
 		countWork(RESTIR_COUNT_PRIMARY, work.nodes, work.triangles);
 		return -1;
 	}
+	// Each entry keeps the box's entry distance: a box that passed its test
+	// when pushed passes it again at the pop exactly when that distance is
+	// still within the nearest hit (its own exit did not change), so the pop
+	// needs no second fetch of the box.
 	int stack[64];
+	float stackEnter[64];
 	int top = 0;
 	int hit = -1;
 	int node = 0;
@@ -402,7 +407,9 @@ __device__ inline int traceNearestFirst(const BvhView& b, V3 o, V3 d, float& dis
 				bool leftFirst = leftDistance <= rightDistance;
 				if (top < 64)
 				{
-					stack[top++] = leftFirst ? right : left;
+					stack[top] = leftFirst ? right : left;
+					stackEnter[top] = leftFirst ? rightDistance : leftDistance;
+					++top;
 				}
 				else
 				{
@@ -421,10 +428,10 @@ __device__ inline int traceNearestFirst(const BvhView& b, V3 o, V3 d, float& dis
 		bool found = false;
 		while (top > 0)
 		{
-			int candidate = stack[--top];
-			if (box(candidate) >= 0.0f)
+			--top;
+			if (stackEnter[top] <= distance)
 			{
-				node = candidate;
+				node = stack[top];
 				found = true;
 				break;
 			}
