@@ -174,6 +174,84 @@ RN_HD float rn_exp(float x)
 	return (p * rn_exp2i(n1)) * rn_exp2i(n2);
 }
 
+#define RN_LN2 6.93147180559945309417e-01f
+#define RN_TWO_OVER_LN2 2.88539008177792681472e+00f
+
+/* log2(x). x = m * 2^e with m in [sqrt(1/2), sqrt(2)), then
+ * log2(m) = (2 / ln 2) * atanh(s), s = (m - 1) / (m + 1), by the series
+ * atanh(s) = s + s^3/3 + ... + s^11/11 (|s| <= 0.172). Zero gives -infinity,
+ * a negative x or NaN gives NaN, +infinity itself. */
+RN_HD float rn_log2(float x)
+{
+	if (!(x > 0.0f))
+	{
+		return x == 0.0f ? rn_bits_float(0xff800000u) : rn_bits_float(0x7fc00000u);
+	}
+	uint32_t bits = rn_float_bits(x);
+	if (bits >= 0x7f800000u)
+	{
+		return x;
+	}
+	int e = 0;
+	if (bits < 0x00800000u)
+	{
+		/* Denormal: scale by 2^23 into the normal range. */
+		bits = rn_float_bits(x * 8388608.0f);
+		e = -23;
+	}
+	e += (int)(bits >> 23) - 127;
+	float m = rn_bits_float((bits & 0x007fffffu) | 0x3f800000u);
+	if (m >= 1.41421356237309504880f)
+	{
+		m = m * 0.5f;
+		e += 1;
+	}
+	float s = (m - 1.0f) / (m + 1.0f);
+	float s2 = s * s;
+	float p = 9.0909090909090909e-02f;   /* 1/11 */
+	p = p * s2 + 1.1111111111111111e-01f; /* 1/9 */
+	p = p * s2 + 1.4285714285714285e-01f; /* 1/7 */
+	p = p * s2 + 2.0000000000000001e-01f; /* 1/5 */
+	p = p * s2 + 3.3333333333333331e-01f; /* 1/3 */
+	p = p * s2 + 1.0f;
+	return (float)e + (s * p) * RN_TWO_OVER_LN2;
+}
+
+/* 2^x: x = k + r with k = round(x), |r| <= 1/2, 2^r = e^(r ln 2) by rn_exp,
+ * then scaling by 2^k in two exact steps as rn_exp does. */
+RN_HD float rn_exp2(float x)
+{
+	if (x != x)
+	{
+		return x;
+	}
+	if (x >= 128.0f)
+	{
+		return rn_bits_float(0x7f800000u);
+	}
+	if (x < -150.0f)
+	{
+		return 0.0f;
+	}
+	float k = rn_round(x);
+	float r = x - k;
+	int n = (int)k;
+	int n1 = n / 2;
+	int n2 = n - n1;
+	return (rn_exp(r * RN_LN2) * rn_exp2i(n1)) * rn_exp2i(n2);
+}
+
+/* x^y for x >= 0 (GLSL's pow, whose result for x < 0 is undefined; callers
+ * pass abs(x) or clamped values): 2^(y log2 x), with 0^y = 0 for y > 0. */
+RN_HD float rn_pow(float x, float y)
+{
+	if (x == 0.0f)
+	{
+		return y > 0.0f ? 0.0f : (y == 0.0f ? 1.0f : rn_bits_float(0x7f800000u));
+	}
+	return rn_exp2(y * rn_log2(x));
+}
+
 /* x^5 and x^64, by a fixed sequence of products (the reference's pow(x, 5.0)
  * and pow(x, 64.0), brdf.sh:460, svgf.sh:203). */
 RN_HD float rn_pow5(float x)
@@ -235,26 +313,20 @@ RN_HD uint16_t rn_float_to_half(float f)
 	return (uint16_t)(sign | half);
 }
 
+/* Exact and branch-free (F. Giesen, "half to float done quic", 2012): the
+ * exponent and mantissa shifted into binary32 position read as a float
+ * 2^-112 times the half's magnitude, denormals included (the product is exact;
+ * it needs denormal operands kept, as both builds do). Infinity and NaN keep
+ * their mantissa bits under an all-ones exponent. */
 RN_HD float rn_half_to_float(uint16_t h)
 {
-	uint32_t sign = ((uint32_t)h & 0x8000u) << 16;
-	uint32_t exp = ((uint32_t)h >> 10) & 0x1fu;
-	uint32_t mant = (uint32_t)h & 0x3ffu;
-	if (exp == 0x1fu)
+	uint32_t shifted = ((uint32_t)h & 0x7fffu) << 13;
+	uint32_t magnitude = rn_float_bits(rn_bits_float(shifted) * 0x1p112f);
+	if (((uint32_t)h & 0x7c00u) == 0x7c00u)
 	{
-		return rn_bits_float(sign | 0x7f800000u | (mant << 13));
+		magnitude = shifted | 0x7f800000u;
 	}
-	if (exp == 0u)
-	{
-		if (mant == 0u)
-		{
-			return rn_bits_float(sign);
-		}
-		/* Denormal: value = mant * 2^-24, exact in binary32. */
-		float v = (float)mant * 5.9604644775390625e-08f;
-		return sign ? -v : v;
-	}
-	return rn_bits_float(sign | ((exp + 112u) << 23) | (mant << 13));
+	return rn_bits_float(magnitude | (((uint32_t)h & 0x8000u) << 16));
 }
 
 /* Unorm8 store and load. */

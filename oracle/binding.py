@@ -12,8 +12,8 @@ from pathlib import Path
 
 import numpy as np
 
-from restir_b200.abi import (RestirDiReservoirs, RestirGBuffer, RestirGiHistory, RestirGiReservoirs, RestirParams,
-                             RestirScene)
+from restir_b200.abi import (RestirDiReservoirs, RestirDisplayParams, RestirGBuffer, RestirGiHistory,
+                             RestirGiReservoirs, RestirParams, RestirScene)
 
 HERE = Path(__file__).resolve().parent
 LIBRARY = HERE / "liboracle.so"
@@ -45,6 +45,9 @@ _SIGNATURES = {
     "oracle_composite": (C.c_int, [PP, PG, P, P, P, P, P]),
     "oracle_reference_accumulate": (C.c_int, [PP, P, P, P, u32]),
     "oracle_error": (C.c_int, [PP, P, P, P, P]),
+    "oracle_exposure": (C.c_int, [C.POINTER(RestirDisplayParams), P, P]),
+    "oracle_taa": (C.c_int, [C.POINTER(RestirDisplayParams), P, P, P, P]),
+    "oracle_tonemap": (C.c_int, [C.POINTER(RestirDisplayParams), P, P, P, P, P]),
     "oracle_last_counts": (None, [P]),
     "oracle_numeric_eval": (None, [C.c_int, P, P, u32]),
     "oracle_grid_keys": (None, [P, P, u32, P, P, P, u32, P, P, P]),

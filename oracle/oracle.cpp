@@ -1634,6 +1634,11 @@ extern "C" void oracle_numeric_eval(int fn, const float* input, float* output, u
 		case 7: y = rn_pow64(x); break;
 		case 8: y = rn_bits_float(pcg(rn_float_bits(x))); break;
 		case 9: y = rn_bits_float(gridChecksumHash(rn_float_bits(x))); break;
+		case 10: y = rn_half_to_float(uint16_t(rn_float_bits(x) & 0xffffu)); break;
+		case 11: y = rn_log2(x); break;
+		case 12: y = rn_exp2(x); break;
+		case 13: y = rn_pow(x, 2.2f); break;
+		case 14: y = rn_pow(x, 1.0f / 2.2f); break;
 		default: break;
 		}
 		output[i] = y;

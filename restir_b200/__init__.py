@@ -21,7 +21,7 @@ import numpy as np
 from . import abi
 from .abi import (RestirBvhDesc, RestirDiReservoirs, RestirFrameInput, RestirFramePlan, RestirFrameState,
                   RestirGBuffer, RestirGiHistory, RestirGiReservoirs, RestirLightsDesc, RestirMeshDesc,
-                  RestirParams, RestirScene, RestirSettings)
+                  RestirParams, RestirScene, RestirSettings, RestirDisplayParams)
 
 # RESTIR_LIBRARY selects another build of the same library (tuning variants).
 LIBRARY_PATH = Path(os.environ.get("RESTIR_LIBRARY", Path(__file__).resolve().parent / "librestir_gpu.so"))
@@ -69,6 +69,13 @@ _SIGNATURES = {
     "restir_error_scratch_bytes": (C.c_uint64, [u32, u32]),
     "restir_error": (C.c_int, [C.POINTER(RestirParams), P, P, P, P, P, P]),
     "restir_error_noalloc": (C.c_int, [C.POINTER(RestirParams), P, P, P, P, P]),
+    # restir_display.h
+    "restir_display_params": (C.c_int, [P, P, u32, u32, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
+                                        C.c_float, C.c_int, C.c_int, C.c_int, C.POINTER(RestirDisplayParams)]),
+    "restir_exposure": (C.c_int, [C.POINTER(RestirDisplayParams), P, P, P]),
+    "restir_taa": (C.c_int, [C.POINTER(RestirDisplayParams), P, P, P, P, P]),
+    "restir_tonemap": (C.c_int, [C.POINTER(RestirDisplayParams), P, P, P, P, P, P]),
+    "restir_display": (C.c_int, [C.POINTER(RestirDisplayParams), P, P, P, P, P, P, P, P, P]),
     "restir_status": (C.c_int, [C.POINTER(u32)]),
     "restir_numeric_eval": (C.c_int, [C.c_int, P, P, u32, P]),
     "restir_counters": (C.c_int, [C.c_int, P]),

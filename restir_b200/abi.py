@@ -135,6 +135,21 @@ class RestirFramePlan(C.Structure):
     ]
 
 
+# --- include/restir_display.h -------------------------------------------------------------------------
+
+TONEMAP_ACES, TONEMAP_AGX, TONEMAP_NEUTRAL, TONEMAP_REINHARD, TONEMAP_CLAMP = range(5)
+
+
+class RestirDisplayParams(C.Structure):
+    _fields_ = [
+        ("inv_view_proj", m16), ("previous_view_proj", m16), ("taa_history_valid", C.c_float),
+        ("origin_bottom_left", C.c_float), ("exposure_adapt", C.c_float), ("exposure_reset", C.c_float),
+        ("exposure_ev", C.c_float), ("auto_exposure", C.c_float), ("tonemapper", C.c_float),
+        ("pass_through", C.c_float), ("reference_view", C.c_float), ("taa", C.c_float),
+        ("width", C.c_uint32), ("height", C.c_uint32),
+    ]
+
+
 # --- include/restir_cache.h ---------------------------------------------------------------------------
 
 CACHE_LEVELS = 16

@@ -118,41 +118,58 @@ __device__ __forceinline__ void unitPosition(const CacheView& c, const float4& q
 	unit[2] = unitCoordinate(q0.z, c.boundsMin[2], c.boundsMax[2]);
 }
 
-// The 64 network inputs of one query as bfloat16, 8 per 16-byte chunk.
+// Two floats as a pair of bfloat16 (lo in the low half).
+__device__ __forceinline__ uint32_t packBf16(float lo, float hi)
+{
+	return uint32_t(rn_float_to_bf16(lo)) | (uint32_t(rn_float_to_bf16(hi)) << 16);
+}
+
+// The 64 network inputs of one query as bfloat16, 8 per 16-byte chunk. The
+// levels are unrolled so that the gathers of all levels can be in flight
+// together; each level still sums its corners in order d = 0..7.
 __device__ inline void queryFeatures(const CacheView& c, const float4* query, uint4 chunk[8])
 {
 	const float4 q0 = query[0], q1 = query[1], q2 = query[2], q3 = query[3];
 	float unit[3];
 	unitPosition(c, q0, unit);
-	uint16_t v[64];
+	uint32_t packed[32];
+#pragma unroll
 	for (int level = 0; level < RESTIR_CACHE_LEVELS; ++level)
 	{
 		LevelCorners corners;
 		levelCorners(c, level, unit, corners);
 		const uint32_t* row = reinterpret_cast<const uint32_t*>(c.tableHalf) + size_t(level) * c.entries;
-		float f0 = 0.0f, f1 = 0.0f;
+		uint32_t pair[8];
+#pragma unroll
 		for (int d = 0; d < 8; ++d)
 		{
-			const uint32_t pair = __ldg(row + corners.index[d]);
-			f0 = f0 + corners.weight[d] * rn_half_to_float(uint16_t(pair & 0xffffu));
-			f1 = f1 + corners.weight[d] * rn_half_to_float(uint16_t(pair >> 16));
+			pair[d] = __ldg(row + corners.index[d]);
 		}
-		v[2 * level] = rn_float_to_bf16(f0);
-		v[2 * level + 1] = rn_float_to_bf16(f1);
+		float f0 = 0.0f, f1 = 0.0f;
+#pragma unroll
+		for (int d = 0; d < 8; ++d)
+		{
+			f0 = f0 + corners.weight[d] * rn_half_to_float(uint16_t(pair[d] & 0xffffu));
+			f1 = f1 + corners.weight[d] * rn_half_to_float(uint16_t(pair[d] >> 16));
+		}
+		packed[level] = packBf16(f0, f1);
 	}
-	const float extra[11] = { q2.x, q2.y, q2.z, q1.x, q1.y, q1.z, q0.w, q3.x, q3.y, q3.z, 1.0f };
-	for (int i = 0; i < 11; ++i)
+	// Inputs 32..42: direction, normal, roughness, albedo, then the constant 1.
+	packed[16] = packBf16(q2.x, q2.y);
+	packed[17] = packBf16(q2.z, q1.x);
+	packed[18] = packBf16(q1.y, q1.z);
+	packed[19] = packBf16(q0.w, q3.x);
+	packed[20] = packBf16(q3.y, q3.z);
+	packed[21] = packBf16(1.0f, 0.0f);
+#pragma unroll
+	for (int i = 22; i < 32; ++i)
 	{
-		v[32 + i] = rn_float_to_bf16(extra[i]);
+		packed[i] = 0u;
 	}
-	for (int i = 43; i < 64; ++i)
-	{
-		v[i] = 0;
-	}
+#pragma unroll
 	for (int k = 0; k < 8; ++k)
 	{
-		chunk[k] = make_uint4(uint32_t(v[8 * k]) | (uint32_t(v[8 * k + 1]) << 16), uint32_t(v[8 * k + 2]) | (uint32_t(v[8 * k + 3]) << 16),
-			uint32_t(v[8 * k + 4]) | (uint32_t(v[8 * k + 5]) << 16), uint32_t(v[8 * k + 6]) | (uint32_t(v[8 * k + 7]) << 16));
+		chunk[k] = make_uint4(packed[4 * k], packed[4 * k + 1], packed[4 * k + 2], packed[4 * k + 3]);
 	}
 }
 
@@ -276,7 +293,7 @@ __device__ __forceinline__ void issueLayer(uint32_t tmemD, const uint8_t* a, con
 constexpr int kForwardSmem = kWeightBytes + kTileBytes + 64;
 
 template<int kMode>  // 0: half4 cache values, 1: 16 raw floats, 2: the 64 inputs
-__global__ void __launch_bounds__(kTile) forwardKernel(CacheView c, const float4* __restrict__ queries, uint32_t n,
+__global__ void __launch_bounds__(kTile, 4) forwardKernel(CacheView c, const float4* __restrict__ queries, uint32_t n,
 	void* __restrict__ output)
 {
 	extern __shared__ __align__(1024) uint8_t smem[];

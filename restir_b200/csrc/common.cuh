@@ -167,13 +167,29 @@ __device__ __forceinline__ V4 loadH4(const uint16_t* p, int i)
 	return { a.x, a.y, b.x, b.y };
 }
 
+// The conversion rounds to nearest even like rn_float_to_half; a NaN becomes
+// that function's quiet NaN (sign | 0x7e00) rather than the converter's
+// canonical one, so that NaN passed through a target keeps the same bits.
+__device__ __forceinline__ uint32_t halfPair(float a, float b)
+{
+	__half2 h = __floats2half2_rn(a, b);
+	uint32_t q = *reinterpret_cast<uint32_t*>(&h);
+	if (a != a)
+	{
+		q = (q & 0xffff0000u) | ((__float_as_uint(a) >> 16) & 0x8000u) | 0x7e00u;
+	}
+	if (b != b)
+	{
+		q = (q & 0x0000ffffu) | (((__float_as_uint(b) >> 16) & 0x8000u) | 0x7e00u) << 16;
+	}
+	return q;
+}
+
 __device__ __forceinline__ void storeH4(uint16_t* p, int i, V4 v)
 {
-	__half2 lo = __floats2half2_rn(v.x, v.y);
-	__half2 hi = __floats2half2_rn(v.z, v.w);
 	uint2 q;
-	q.x = *reinterpret_cast<uint32_t*>(&lo);
-	q.y = *reinterpret_cast<uint32_t*>(&hi);
+	q.x = halfPair(v.x, v.y);
+	q.y = halfPair(v.z, v.w);
 	reinterpret_cast<uint2*>(p)[i] = q;
 }
 

@@ -29,6 +29,11 @@ __global__ void numericKernel(int fn, const float* __restrict__ in, float* __res
 	case 7: y = rn_pow64(x); break;
 	case 8: y = __uint_as_float(pcg(__float_as_uint(x))); break;
 	case 9: y = __uint_as_float(gridChecksumHash(__float_as_uint(x))); break;
+	case 10: y = rn_half_to_float(uint16_t(__float_as_uint(x) & 0xffffu)); break;
+	case 11: y = rn_log2(x); break;
+	case 12: y = rn_exp2(x); break;
+	case 13: y = rn_pow(x, 2.2f); break;
+	case 14: y = rn_pow(x, 1.0f / 2.2f); break;
 	default: y = x; break;
 	}
 	out[i] = y;

@@ -160,3 +160,69 @@ def grid_cells(grid: np.ndarray, table_size: int, capacity: int) -> dict:
         c = int(counts[slot])
         cells[int(checks[slot])] = (c, entries[slot, :min(c, capacity)].copy())
     return cells
+
+
+# --- display passes (include/restir_display.h) -------------------------------------------------------------------
+
+def perspective_view_proj(eye, target, aspect: float, fov_y: float = 1.0, near: float = 0.05, far: float = 50.0):
+    """A row-major view-projection (clip = M v, NDC depth in [0, 1]) and its inverse, float32."""
+    eye = np.asarray(eye, np.float64)
+    forward = np.asarray(target, np.float64) - eye
+    forward /= np.linalg.norm(forward)
+    right = np.cross(forward, [0.0, 1.0, 0.0])
+    right /= np.linalg.norm(right)
+    up = np.cross(right, forward)
+    view = np.eye(4)
+    view[0, :3], view[1, :3], view[2, :3] = right, up, forward
+    view[:3, 3] = -view[:3, :3] @ eye
+    f = 1.0 / np.tan(fov_y / 2.0)
+    proj = np.zeros((4, 4))
+    proj[0, 0], proj[1, 1] = f / aspect, f
+    proj[2, 2], proj[2, 3] = far / (far - near), -near * far / (far - near)
+    proj[3, 2] = 1.0
+    vp = proj @ view
+    return vp.astype(np.float32), np.linalg.inv(vp).astype(np.float32)
+
+
+def half_image(values: np.ndarray) -> np.ndarray:
+    """float (h, w, 4) -> RGBA16F bits (h * w * 4 uint16)."""
+    return np.ascontiguousarray(values.astype(np.float16)).view(np.uint16).reshape(-1)
+
+
+def display_inputs(width: int, height: int, seed: int = 0, specials: bool = True):
+    """Seeded display-pass inputs: an HDR composite with background pixels
+    (alpha 0), a depth buffer (1 on the background), last frame's TAA output,
+    and matrices of a camera that moved a little since last frame."""
+    rng = np.random.default_rng(seed)
+    hdr = np.empty((height, width, 4), np.float32)
+    hdr[..., :3] = rng.lognormal(-1.0, 1.5, (height, width, 3))
+    background = rng.random((height, width)) < 0.15
+    hdr[..., 3] = np.where(background, 0.0, 1.0)
+    depth = np.where(background, 1.0, rng.uniform(0.90, 0.999, (height, width))).astype(np.float32)
+    if specials:
+        hdr[0, 0, :3] = np.inf
+        hdr[height // 2, width // 3, 1] = np.nan
+        hdr[height - 1, width - 1, :3] = 6.0e4
+    history = np.empty((height, width, 4), np.float32)
+    history[..., :3] = rng.lognormal(-1.0, 1.5, (height, width, 3))
+    history[..., 3] = hdr[..., 3]
+    aspect = width / height
+    vp, inv = perspective_view_proj([0.3, 0.5, -3.0], [0.0, 0.0, 0.0], aspect)
+    previous, _ = perspective_view_proj([0.33, 0.49, -3.02], [0.01, 0.0, 0.0], aspect)
+    return {"hdr": half_image(hdr), "depth": depth.reshape(-1), "history": half_image(history),
+            "inv_view_proj": inv, "previous_view_proj": previous, "view_proj": vp}
+
+
+def display_params(width: int, height: int, inputs: dict, **fields):
+    from restir_b200.abi import RestirDisplayParams
+    p = RestirDisplayParams()
+    p.inv_view_proj[:] = [float(v) for v in inputs["inv_view_proj"].reshape(-1)]
+    p.previous_view_proj[:] = [float(v) for v in inputs["previous_view_proj"].reshape(-1)]
+    p.width, p.height = width, height
+    p.taa_history_valid = 1.0
+    p.exposure_adapt = 0.05
+    p.tonemapper = 1.0
+    p.taa = 1.0
+    for name, value in fields.items():
+        setattr(p, name, value)
+    return p

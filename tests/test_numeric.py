@@ -39,6 +39,40 @@ def test_half_round_trip_matches_numpy():
     np.testing.assert_array_equal(host_eval(4, x).view(np.uint32), ref.view(np.uint32))
 
 
+def test_half_to_float_exhaustive():
+    # Every binary16 pattern (denormals, infinities and NaN payloads included)
+    # against numpy's widening, bit for bit.
+    bits = np.arange(65536, dtype=np.uint32)
+    out = host_eval(10, bits.view(np.float32).copy())
+    expected = bits.astype(np.uint16).view(np.float16).astype(np.float32)
+    np.testing.assert_array_equal(out.view(np.uint32), expected.view(np.uint32))
+
+
+def test_log2_exp2_pow_accuracy():
+    # The display passes' transcendental functions (auto exposure's log2,
+    # tone mapping's exp2 and pow): a few ulps against float64.
+    x = np.concatenate([np.geomspace(1e-44, 3e38, 200001).astype(np.float32),
+                        np.linspace(0.5, 2.0, 50001, dtype=np.float32)])
+    y = host_eval(11, x).astype(np.float64)
+    ref = np.log2(x.astype(np.float64))
+    assert np.max(np.abs(y - ref) / np.spacing(np.abs(ref).astype(np.float32))) < 4.0
+    special = host_eval(11, np.array([0.0, -1.0, np.inf, np.nan, 1.0, 0.5], np.float32))
+    assert special[0] == -np.inf and np.isnan(special[1]) and special[2] == np.inf and np.isnan(special[3])
+    assert special[4] == 0.0 and special[5] == -1.0
+    x = np.linspace(-160.0, 130.0, 400001, dtype=np.float32)
+    y = host_eval(12, x).astype(np.float64)
+    ref = np.exp2(x.astype(np.float64))
+    normal = (ref > 1.2e-38) & (ref < 3.0e38)
+    assert np.max(np.abs(y[normal] / ref[normal] - 1.0)) < 2e-7
+    assert np.all(host_eval(12, np.array([-200.0, 0.0, 1.0, 128.0], np.float32)) == np.array([0.0, 1.0, 2.0, np.inf], np.float32))
+    x = np.linspace(0.0, 4.0, 100001, dtype=np.float32)
+    for fn, e in ((13, 2.2), (14, 1.0 / 2.2)):
+        y = host_eval(fn, x).astype(np.float64)
+        ref = x.astype(np.float64) ** e
+        assert y[0] == 0.0
+        assert np.max(np.abs(y[1:] / ref[1:] - 1.0)) < 4e-6
+
+
 def test_unorm8_and_log2():
     x = np.linspace(-0.1, 1.1, 1201, dtype=np.float32)
     expected = np.round(np.clip(x, 0, 1).astype(np.float64) * 255.0 + 1e-9)
@@ -61,6 +95,11 @@ def test_device_numeric_bit_identical():
         5: np.linspace(-0.1, 1.1, 100003, dtype=np.float32),
         6: np.abs(rng.normal(size=100003).astype(np.float32)) * 1000.0 + 1.0,
         7: rng.random(100003).astype(np.float32),
+        10: np.arange(65536, dtype=np.uint32).view(np.float32),
+        11: np.geomspace(1e-44, 3e38, 100003).astype(np.float32),
+        12: np.linspace(-160.0, 130.0, 100003, dtype=np.float32),
+        13: np.linspace(0.0, 4.0, 100003, dtype=np.float32),
+        14: np.linspace(0.0, 4.0, 100003, dtype=np.float32),
     }
     lib = rb.load()
     for fn, x in inputs.items():
