@@ -6,10 +6,10 @@
  * and runs the passes in the reference's order on one CUDA stream
  * (optionally replayed from a CUDA graph).
  *
- * Scope: the passes named in restir_gpu.h. TAA, auto exposure, tone
- * mapping, specular GI and the debug views are not part of this driver;
- * their settings are fixed off (TAA off also means the camera is jittered
- * only while the reference accumulates, renderer.cpp:472-488).
+ * Scope: the passes named in restir_gpu.h and the display chain of
+ * restir_display.h (auto exposure, TAA, tone mapping into a BGRA8 image).
+ * Specular GI and the debug views are not part of this driver; their
+ * settings are fixed off.
  */
 #ifndef RESTIR_FRAME_H
 #define RESTIR_FRAME_H
@@ -69,6 +69,14 @@ typedef struct RestirSettings
 	uint32_t cache_training_samples;  /* path suffixes per frame (default 65,536) */
 	uint32_t wave_visibility;         /* 1: visibility rays in warp lock step (traceBvhWave,
 	                                     bvh.sh:177-212, the reference's Vulkan path) */
+	int taa;                 /* temporal anti-aliasing: jittered frames blended in the TAA
+	                            pass (settings.h:194) */
+	int auto_exposure;       /* settings.h:214 */
+	int tonemapper;          /* RESTIR_TONEMAP_* (settings.h:212) */
+	float exposure_ev;       /* settings.h:213 */
+	float adaptation_speed;  /* settings.h:215, per second */
+	int display;             /* no reference counterpart (the reference always draws to its
+	                            window): 0 skips exposure, TAA and tone mapping */
 } RestirSettings;
 
 /* FrameInput (renderer.h) with the fly camera's pose. */
@@ -77,6 +85,7 @@ typedef struct RestirFrameInput
 	uint32_t width, height;
 	float eye[3];
 	float yaw, pitch;
+	float delta_time;        /* FrameInput::m_deltaTime, seconds (auto exposure's adaptation) */
 } RestirFrameInput;
 
 /* What Renderer carries from frame to frame. */
@@ -89,6 +98,9 @@ typedef struct RestirFrameState
 	float previous_eye[3];
 	int reference_accumulating;
 	uint32_t reference_frames;
+	float previous_unjittered_view_proj[16]; /* m_previousUnjitteredViewProj (TAA) */
+	int taa_valid;                           /* m_taaValid */
+	int exposure_valid;                      /* m_exposureValid */
 } RestirFrameState;
 
 /* Which passes the frame runs. */
@@ -100,6 +112,10 @@ typedef struct RestirFramePlan
 	int reference_accumulate;     /* the reference accumulates this frame */
 	uint32_t reference_weight_frames; /* frames in the mean before this one */
 	int surface_light_is_di;      /* GI reads the DI diffuse (else the G-buffer emission) */
+	int display;                  /* the display chain runs (settings.display) */
+	int taa;                      /* TAA runs: settings.taa, not while the reference accumulates */
+	int exposure;                 /* auto exposure runs */
+	float unjittered_view_proj[16]; /* this frame's, for the next frame's TAA */
 } RestirFramePlan;
 
 void restir_settings_default(RestirSettings* settings);
@@ -130,7 +146,8 @@ void restir_frame_advance(const RestirParams* params, const RestirFramePlan* pla
 #define RESTIR_PASS_COMPOSITE 8
 #define RESTIR_PASS_REFERENCE 9
 #define RESTIR_PASS_CACHE 10      /* radiance-cache training (no reference counterpart) */
-#define RESTIR_PASS_COUNT 11
+#define RESTIR_PASS_DISPLAY 11    /* auto exposure, TAA and tone mapping */
+#define RESTIR_PASS_COUNT 12
 
 typedef struct RestirMetrics
 {

@@ -355,6 +355,12 @@ int restir_error(const RestirParams* params, const uint16_t* display, const doub
 int restir_error_noalloc(const RestirParams* params, const uint16_t* display, const double* mean,
 	const uint8_t* alpha, double* out, void* stream);
 
+/* The byte size of a public struct of this ABI by its name ("RestirParams",
+ * "RestirSettings", ...; every struct of the include/ headers), 0 for an
+ * unknown name: a binding in another language checks its copies of the
+ * layouts against it. Host only. */
+uint64_t restir_struct_size(const char* name);
+
 /* Reads and clears the device status word: bit 0 a traversal reached its
  * step cap, bit 1 a hash grid probe sequence was exhausted, bit 2 a ray
  * queue was full (rays past its capacity are not traced), bit 3 a

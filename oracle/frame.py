@@ -40,6 +40,8 @@ LAYOUT = {
     "filter0": (np.uint16, 4, "gi"), "filter1": (np.uint16, 4, "gi"),
     "hdr": (np.uint16, 4, "full"),
     "ref.mean": (np.float64, 3, "full"), "ref.alpha": (np.uint8, 1, "full"),
+    "taa0": (np.uint16, 4, "full"), "taa1": (np.uint16, 4, "full"), "display": (np.uint8, 4, "full"),
+    "exposure": (np.uint32, 1, "one"),
 }
 
 
@@ -56,13 +58,15 @@ class FrameRunner:
         self.state = rb.initial_state()
         self.history_read = 0
         self.di_read = 0
+        self.taa_read = 0
+        self.display_taa = False
         self.params = None
         self.plan = None
         self.frame_input = rb.frame_input(setup.mesh, width, height)
         p, _ = rb.frame_params(self.settings, setup.mesh, setup.lights.count, setup.bvh, self.frame_input, self.state)
         self.shape = {"full": width * height, "gi": p.gi_width * p.gi_height,
                       "atlas": 6 * p.shadow_face_size * p.shadow_face_size,
-                      "grid": p.grid_table_size * (2 + p.grid_cell_capacity)}
+                      "grid": p.grid_table_size * (2 + p.grid_cell_capacity), "one": 1}
         self.buffers = {}
         for name, (dt, ch, res) in LAYOUT.items():
             n = self.shape[res] * ch
@@ -187,7 +191,33 @@ class FrameRunner:
             out.append(("reference_accumulate", lambda: self.call(
                 "reference_accumulate", P, self.b("hdr"), self.b("ref.mean"), self.b("ref.alpha"),
                 plan.reference_weight_frames)))
+        if plan.display:
+            # Auto exposure, TAA and tone mapping (renderer.cpp:987-1117), as three passes.
+            D = self.display_params()
+            taa_read, taa_write = self.b(f"taa{self.taa_read}"), self.b(f"taa{1 - self.taa_read}")
+            if plan.exposure:
+                out.append(("exposure", lambda: self.call("exposure", C.byref(D), self.b("hdr"), self.b("exposure"))))
+            if plan.taa:
+                out.append(("taa", lambda: self.call("taa", C.byref(D), self.b("hdr"), self.b("gb.depth"), taa_read,
+                                                     taa_write)))
+            shown = taa_write if plan.taa else self.b("hdr")
+            out.append(("tonemap", lambda: self.call("tonemap", C.byref(D), shown, self.b("exposure"), None, None,
+                                                     self.b("display"))))
         return out
+
+    def display_params(self):
+        """The display passes' uniforms from the library's host code (restir_display_params)."""
+        from restir_b200.abi import RestirDisplayParams
+        P, plan, s = self.params, self.plan, self.settings
+        D = RestirDisplayParams()
+        inv = (C.c_float * 16)(*P.inv_view_proj)
+        previous = (C.c_float * 16)(*self.state.previous_unjittered_view_proj)
+        rb.check(rb.load().restir_display_params(C.cast(inv, C.c_void_p), C.cast(previous, C.c_void_p), P.width, P.height,
+                                                 plan.taa, self.state.taa_valid, plan.exposure,
+                                                 self.state.exposure_valid, s.adaptation_speed,
+                                                 self.frame_input.delta_time, s.exposure_ev, s.tonemapper, 0, 0,
+                                                 C.byref(D)), "display_params")
+        return D
 
     def gi_temporal_wavefront(self, P, gb, history, grid, surface, current):
         import torch
@@ -228,6 +258,9 @@ class FrameRunner:
     def finish(self):
         rb.advance(self.params, self.plan, self.frame_input, self.state)
         self.history_read = 1 - self.history_read
+        self.display_taa = bool(self.plan.display and self.plan.taa)
+        if self.display_taa:
+            self.taa_read = 1 - self.taa_read
         if self.plan.di_active:
             self.di_read = 1 - self.di_read
 
@@ -248,6 +281,11 @@ class FrameRunner:
         if accumulate:
             self.state.reference_frames = 0
         self.state.history_valid = 0
+        self.state.taa_valid = 0
+
+    def displayed(self) -> str:
+        """The buffer the last frame displayed: its TAA output, or the composite."""
+        return f"taa{self.taa_read}" if self.display_taa else "hdr"
 
     def error(self) -> np.ndarray:
         """cs_error.sc against the reference, FP64: relMSE, mean image, mean reference, count."""
@@ -259,11 +297,11 @@ class FrameRunner:
                 nbytes = self.lib.restir_error_scratch_bytes(self.width, self.height)
                 self.error_scratch = torch.zeros(nbytes // 8 + 1, dtype=torch.float64, device="cuda")
             d = torch.zeros(4, dtype=torch.float64, device="cuda")
-            rb.check(self.lib.restir_error(P, self.b("hdr"), self.b("ref.mean"), self.b("ref.alpha"), d.data_ptr(),
+            rb.check(self.lib.restir_error(P, self.b(self.displayed()), self.b("ref.mean"), self.b("ref.alpha"), d.data_ptr(),
                                            self.error_scratch.data_ptr(), None), "error")
             out[:] = d.cpu().numpy()
         else:
-            rb.check(self.lib.oracle_error(P, self.b("hdr"), self.b("ref.mean"), self.b("ref.alpha"),
+            rb.check(self.lib.oracle_error(P, self.b(self.displayed()), self.b("ref.mean"), self.b("ref.alpha"),
                                            out.ctypes.data), "error")
         return out
 

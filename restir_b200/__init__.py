@@ -35,7 +35,7 @@ ERROR_TIMEOUT, ERROR_OUT_OF_MEMORY, ERROR_TOO_LARGE = -5, -6, -7
 TRACE_CLOSEST, TRACE_ANY, TRACE_CLOSEST_STACKLESS, TRACE_CLOSEST_WATERTIGHT, TRACE_CLOSEST_QUEUE = 0, 1, 2, 3, 4
 TRACE_ANY_WAVE = 5
 PASS_NAMES = ["shadow", "gbuffer", "di_temporal", "di_spatial", "grid", "gi_temporal", "gi_spatial",
-              "denoise", "composite", "reference", "cache"]
+              "denoise", "composite", "reference", "cache", "display"]
 
 _lib = None
 
@@ -76,6 +76,7 @@ _SIGNATURES = {
     "restir_taa": (C.c_int, [C.POINTER(RestirDisplayParams), P, P, P, P, P]),
     "restir_tonemap": (C.c_int, [C.POINTER(RestirDisplayParams), P, P, P, P, P, P]),
     "restir_display": (C.c_int, [C.POINTER(RestirDisplayParams), P, P, P, P, P, P, P, P, P]),
+    "restir_struct_size": (C.c_uint64, [C.c_char_p]),
     "restir_status": (C.c_int, [C.POINTER(u32)]),
     "restir_numeric_eval": (C.c_int, [C.c_int, P, P, u32, P]),
     "restir_counters": (C.c_int, [C.c_int, P]),
@@ -300,12 +301,15 @@ def initial_state() -> RestirFrameState:
     state = RestirFrameState()
     for i in range(4):
         state.previous_view_proj[i * 5] = 1.0
+        state.previous_unjittered_view_proj[i * 5] = 1.0
     return state
 
 
-def frame_input(mesh: Mesh, width: int, height: int, eye=None, yaw=None, pitch=None) -> RestirFrameInput:
+def frame_input(mesh: Mesh, width: int, height: int, eye=None, yaw=None, pitch=None,
+                delta_time: float = 1.0 / 60.0) -> RestirFrameInput:
     fi = RestirFrameInput()
     fi.width, fi.height = width, height
+    fi.delta_time = delta_time
     e = eye if eye is not None else mesh.desc.camera_eye
     for k in range(3):
         fi.eye[k] = e[k]
@@ -392,6 +396,13 @@ class Renderer:
         check(self._lib.restir_renderer_last_frame(self.handle, C.byref(params), C.byref(plan), C.byref(state)),
               "last_frame")
         return params, plan, state
+
+    def display_image(self) -> np.ndarray:
+        """The last frame's tone-mapped image, (height, width, 4) RGBA bytes."""
+        params, _, _ = self.last_frame()
+        n = params.width * params.height * 4
+        bgra = self.download("display", np.uint8)[:n].reshape(params.height, params.width, 4)
+        return bgra[..., [2, 1, 0, 3]].copy()
 
     def buffer(self, name: str) -> tuple[int, int]:
         pointer, nbytes = C.c_void_p(), C.c_uint64()

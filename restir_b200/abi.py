@@ -105,25 +105,28 @@ class RestirSettings(C.Structure):
         ("grid_table_size", C.c_uint32), ("grid_cell_capacity", C.c_uint32), ("grid_mode", C.c_uint32),
         ("wavefront", C.c_uint32), ("radiance_cache", C.c_uint32), ("cache_training_samples", C.c_uint32),
         ("wave_visibility", C.c_uint32),
+        ("taa", C.c_int), ("auto_exposure", C.c_int), ("tonemapper", C.c_int), ("exposure_ev", C.c_float),
+        ("adaptation_speed", C.c_float), ("display", C.c_int),
     ]
 
 
 class RestirFrameInput(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("eye", f3), ("yaw", C.c_float),
-                ("pitch", C.c_float)]
+                ("pitch", C.c_float), ("delta_time", C.c_float)]
 
 
 class RestirFrameState(C.Structure):
     _fields_ = [
         ("frame_number", C.c_uint32), ("history_valid", C.c_int), ("di_valid", C.c_int),
         ("previous_view_proj", m16), ("previous_eye", f3), ("reference_accumulating", C.c_int),
-        ("reference_frames", C.c_uint32),
+        ("reference_frames", C.c_uint32), ("previous_unjittered_view_proj", m16), ("taa_valid", C.c_int),
+        ("exposure_valid", C.c_int),
     ]
 
 
 class RestirMetrics(C.Structure):
     _fields_ = [("valid", C.c_int), ("relative_mse", C.c_double), ("bias", C.c_double), ("error", C.c_double * 4),
-                ("pass_ms", C.c_float * 11), ("reference_frames", C.c_uint32)]
+                ("pass_ms", C.c_float * 12), ("reference_frames", C.c_uint32)]
 
 
 class RestirFramePlan(C.Structure):
@@ -131,7 +134,8 @@ class RestirFramePlan(C.Structure):
     _fields_ = [
         ("di_active", C.c_int), ("denoiser", C.c_int), ("atrous_iterations", C.c_int),
         ("reference_accumulate", C.c_int), ("reference_weight_frames", C.c_uint32),
-        ("surface_light_is_di", C.c_int),
+        ("surface_light_is_di", C.c_int), ("display", C.c_int), ("taa", C.c_int), ("exposure", C.c_int),
+        ("unjittered_view_proj", m16),
     ]
 
 

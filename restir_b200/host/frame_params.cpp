@@ -2,6 +2,7 @@
 // (src/renderer.cpp:435-731), and the state it carries to the next
 // (renderer.cpp:1119-1124).
 #include "../../include/restir_cache.h"
+#include "../../include/restir_display.h"
 #include "../../include/restir_frame.h"
 #include "bvh_build.h"
 
@@ -18,6 +19,7 @@ constexpr int kShadowFaceBorder = 4;
 constexpr float kGridMinCellSize = 0.02f;
 constexpr float kGridCellPixels = 6.0f;
 constexpr uint32_t kReferenceJitterCount = 1024;
+constexpr uint32_t kTaaJitterCount = 8;
 constexpr float kJacobianClamp = 10.0f;
 constexpr float kOutlierClamp = 8.0f;
 constexpr float kBoilingFilter = 4.0f;
@@ -85,6 +87,12 @@ extern "C" void restir_settings_default(RestirSettings* s)
 	s->radiance_cache = 0;
 	s->cache_training_samples = 65536;
 	s->wave_visibility = 0;
+	s->taa = 1;
+	s->auto_exposure = 0;
+	s->tonemapper = RESTIR_TONEMAP_AGX;
+	s->exposure_ev = 0.0f;
+	s->adaptation_speed = 1.5f;
+	s->display = 1;
 }
 
 extern "C" int restir_frame_params(const RestirSettings* requested, const RestirMeshDesc* scene, uint32_t light_count,
@@ -120,10 +128,14 @@ extern "C" int restir_frame_params(const RestirSettings* requested, const Restir
 	restir_camera_matrices(input->eye, input->yaw, input->pitch, float(width) / float(height), center, radius, view, projection);
 	float unjittered[16];
 	restir::multiply(projection, view, unjittered);
-	if (state->reference_accumulating)
+	// TAA integrates a Halton (2, 3) sub-pixel jitter over 8 frames; the
+	// reference accumulation over 1024 (renderer.cpp:472-488). The scene passes
+	// use the jittered matrices, TAA reprojects with the unjittered ones.
+	const bool taa = s.taa != 0 && s.display != 0 && !state->reference_accumulating;
+	if (taa || state->reference_accumulating)
 	{
-		// Halton (2, 3) sub-pixel jitter over 1024 frames: clip.xy += jitter * clip.w.
-		const uint32_t index = (state->frame_number % kReferenceJitterCount) + 1;
+		// clip.xy += jitter * clip.w.
+		const uint32_t index = (state->frame_number % (state->reference_accumulating ? kReferenceJitterCount : kTaaJitterCount)) + 1;
 		const float jitterX = (halton(index, 2) - 0.5f) * 2.0f / float(width);
 		const float jitterY = (halton(index, 3) - 0.5f) * 2.0f / float(height);
 		for (int c = 0; c < 4; ++c)
@@ -243,6 +255,10 @@ extern "C" int restir_frame_params(const RestirSettings* requested, const Restir
 		plan->reference_accumulate = state->reference_accumulating ? 1 : 0;
 		plan->reference_weight_frames = state->reference_frames;
 		plan->surface_light_is_di = restirDi ? 1 : 0;
+		plan->display = s.display ? 1 : 0;
+		plan->taa = taa ? 1 : 0;
+		plan->exposure = s.display && s.auto_exposure ? 1 : 0;
+		copy16(plan->unjittered_view_proj, unjittered);
 	}
 	return RESTIR_OK;
 }
@@ -263,5 +279,12 @@ extern "C" void restir_frame_advance(const RestirParams* params, const RestirFra
 	if (state->reference_accumulating)
 	{
 		state->reference_frames += 1;
+	}
+	// TAA and auto exposure history (renderer.cpp:1004-1045, 1120).
+	if (plan != nullptr)
+	{
+		copy16(state->previous_unjittered_view_proj, plan->unjittered_view_proj);
+		state->taa_valid = plan->taa;
+		state->exposure_valid = plan->exposure;
 	}
 }

@@ -9,6 +9,7 @@
 // captured again and patched into the instantiated graph
 // (cudaGraphExecUpdate), since their uniforms and ping-pong buffers change.
 #include "../../include/restir_cache.h"
+#include "../../include/restir_display.h"
 #include "../../include/restir_frame.h"
 #include "bvh_build.h"
 
@@ -127,6 +128,8 @@ public:
 		m_state.history_valid = 0;
 		m_state.di_valid = 0;
 		m_state.reference_frames = 0;
+		m_state.taa_valid = 0;
+		m_state.exposure_valid = 0;
 		m_scene->has = status == 0;
 		return status == 0 ? RESTIR_OK : RESTIR_ERROR_OUT_OF_MEMORY;
 	}
@@ -178,12 +181,16 @@ public:
 		bvhDesc.triangle_offset = m_scene->bvh.triangleOffset;
 		bvhDesc.triangle_count = m_scene->bvh.triangleCount;
 		// Reference mode: a moved camera starts the reference again (renderer.cpp:1050-1060).
+		// The frame time is not part of the view.
+		RestirFrameInput view = input;
+		view.delta_time = 0.0f;
 		if (m_state.reference_accumulating && m_state.reference_frames > 0
-			&& (std::memcmp(&m_referenceInput, &input, sizeof(input)) != 0))
+			&& (std::memcmp(&m_referenceInput, &view, sizeof(view)) != 0))
 		{
 			m_state.reference_frames = 0;
 		}
-		m_referenceInput = input;
+		m_referenceInput = view;
+		m_deltaTime = input.delta_time;
 		status = restir_frame_params(&m_settings, &desc, m_scene->lights.count, &bvhDesc, &input, &m_state, &m_params, &m_plan);
 		if (status != RESTIR_OK)
 		{
@@ -210,6 +217,11 @@ public:
 	{
 		restir_frame_advance(&m_params, &m_plan, &input, &m_state);
 		m_historyRead = 1 - m_historyRead;
+		m_displayTaa = m_plan.display && m_plan.taa;
+		if (m_displayTaa)
+		{
+			m_taaRead = 1 - m_taaRead;
+		}
 		if (m_plan.di_active)
 		{
 			m_diRead = 1 - m_diRead;
@@ -255,6 +267,8 @@ public:
 		m_state.history_valid = 0;
 		m_state.di_valid = 0;
 		m_state.reference_frames = 0;
+		m_state.taa_valid = 0;
+		m_state.exposure_valid = 0;
 	}
 
 	// The batch's shadow atlas and ray queue (null: the renderer's own).
@@ -319,7 +333,8 @@ public:
 		{
 			return RESTIR_ERROR_INVALID_ARGUMENT;
 		}
-		int status = launchError(&m_params, p<uint16_t>("hdr"), p<double>("reference.mean"), p<uint8_t>("reference.alpha"),
+		// The error pass compares the displayed image: the TAA output when TAA ran (renderer.cpp:1078-1094).
+		int status = launchError(&m_params, displayedHdr(), p<double>("reference.mean"), p<uint8_t>("reference.alpha"),
 			p<double>("error.out"), p<double>("error.scratch"), m_stream);
 		if (status != RESTIR_OK)
 		{
@@ -387,7 +402,9 @@ public:
 		{
 			m_state.reference_frames = 0;
 		}
+		// The history means something else with and without the shortcuts (renderer.cpp:1139-1141).
 		m_state.history_valid = 0;
+		m_state.taa_valid = 0;
 	}
 
 	void invalidateHistory()
@@ -426,8 +443,20 @@ public:
 		}
 	}
 
+	// The last frame's displayed HDR image: its TAA output, or the composite.
+	uint16_t* displayedHdr()
+	{
+		return m_displayTaa ? p<uint16_t>("taa" + std::to_string(m_taaRead)) : p<uint16_t>("hdr");
+	}
+
 	int buffer(const std::string& name, void** pointer, uint64_t* bytes)
 	{
+		if (name == "display.hdr" && !m_targets.empty())
+		{
+			*pointer = displayedHdr();
+			*bytes = m_targets["hdr"].bytes;
+			return RESTIR_OK;
+		}
 		auto it = m_targets.find(name);
 		if (it == m_targets.end())
 		{
@@ -543,6 +572,7 @@ private:
 			{ "gi.color0", gi * 8 }, { "gi.color1", gi * 8 }, { "gi.moments0", gi * 8 }, { "gi.moments1", gi * 8 },
 			{ "filtered0", gi * 8 }, { "filtered1", gi * 8 }, { "filter0", gi * 8 }, { "filter1", gi * 8 },
 			{ "hdr", full * 8 }, { "reference.mean", full * 24 }, { "reference.alpha", full },
+			{ "taa0", full * 8 }, { "taa1", full * 8 }, { "display", full * 4 }, { "exposure", 64 },
 			{ "error.scratch", errorScratchBytes() }, { "error.out", 64 },
 		};
 		for (const Spec& s : specs)
@@ -559,10 +589,14 @@ private:
 		}
 		m_historyRead = 0;
 		m_diRead = 0;
+		m_taaRead = 0;
+		m_displayTaa = false;
 		m_state.history_valid = 0;
 		m_state.di_valid = 0;
 		m_state.reference_frames = 0;
 		m_state.frame_number = 0;
+		m_state.taa_valid = 0;
+		m_state.exposure_valid = 0;
 		std::memset(m_state.previous_view_proj, 0, sizeof(m_state.previous_view_proj));
 		for (int i = 0; i < 4; ++i)
 		{
@@ -775,6 +809,19 @@ private:
 					p<uint8_t>("reference.alpha"), plan.reference_weight_frames, s);
 			});
 		}
+		if (plan.display)
+		{
+			// Auto exposure, TAA and tone mapping (renderer.cpp:987-1117).
+			RestirDisplayParams D;
+			status |= restir_display_params(P.inv_view_proj, m_state.previous_unjittered_view_proj, P.width, P.height,
+				plan.taa, m_state.taa_valid, plan.exposure, m_state.exposure_valid, m_settings.adaptation_speed,
+				m_deltaTime, m_settings.exposure_ev, m_settings.tonemapper, 0, 0, &D);
+			const std::string taaRead = "taa" + std::to_string(m_taaRead), taaWrite = "taa" + std::to_string(1 - m_taaRead);
+			run(RESTIR_PASS_DISPLAY, [&] {
+				return restir_display(&D, p<uint16_t>("hdr"), p<float>("gbuffer.depth"), p<uint16_t>(taaRead),
+					p<uint16_t>(taaWrite), p<uint32_t>("exposure"), nullptr, nullptr, p<uint8_t>("display"), s);
+			});
+		}
 		return status == RESTIR_OK ? RESTIR_OK : RESTIR_ERROR_LAUNCH;
 	}
 
@@ -854,6 +901,9 @@ private:
 	uint32_t m_width = 0, m_height = 0, m_giWidth = 0, m_giHeight = 0, m_faceSize = 0, m_tableSize = 0, m_capacity = 0;
 	int m_historyRead = 0;
 	int m_diRead = 0;
+	float m_deltaTime = 0.0f; // the frame input's delta_time (auto exposure)
+	int m_taaRead = 0;        // the TAA target holding last frame's output
+	bool m_displayTaa = false; // the last frame's displayed HDR is its TAA output
 	bool m_timed = false;
 	// Per-pass events of the last kEventRing stream-launched frames.
 	static constexpr uint32_t kEventRing = 128;

@@ -38,3 +38,16 @@ def test_binding_has_a_signature_for_every_declared_function():
     known = set(rb._SIGNATURES)
     missing = [(h, n) for h, fns in declared().items() for n in fns if n not in known]
     assert not missing, missing
+
+
+def test_struct_layouts_match_the_binding():
+    import ctypes as C
+
+    from restir_b200 import abi
+    lib = rb.load()
+    structs = {name: obj for name, obj in vars(abi).items()
+               if name.startswith("Restir") and isinstance(obj, type) and issubclass(obj, C.Structure)}
+    assert len(structs) >= 19
+    for name, cls in structs.items():
+        assert lib.restir_struct_size(name.encode()) == C.sizeof(cls), name
+    assert lib.restir_struct_size(b"NoSuchStruct") == 0

@@ -152,3 +152,32 @@ def test_display_rejects_bad_arguments():
         == rb.ERROR_INVALID_ARGUMENT
     p.width = 0
     assert lib.restir_exposure(C.byref(p), hdr.data_ptr(), out.data_ptr(), None) == rb.ERROR_INVALID_ARGUMENT
+
+
+def test_renderer_display_chain_equals_pass_by_pass_frames():
+    """The frame driver's fused display launch and TAA ping-pong against the
+    same frames run pass by pass (FrameRunner, separate exposure, TAA and
+    tone-mapping calls), with auto exposure on."""
+    from oracle.frame import FrameRunner
+    from helpers import make_scene
+    setup = make_scene(rb.SCENE_CORNELL)
+    settings = setup.settings
+    settings.gi_divisor = 1
+    settings.grid_mode = rb.GRID_DETERMINISTIC
+    settings.auto_exposure = 1
+    w, h = 72, 40
+    runner = FrameRunner(setup, w, h, "cuda", settings)
+    renderer = rb.Renderer(settings)
+    renderer.set_scene(setup.mesh, use_scene_defaults=False)
+    frame = rb.frame_input(setup.mesh, w, h)
+    for _ in range(4):
+        runner.render()
+        renderer.render(frame)
+    _, plan, state = renderer.last_frame()
+    assert plan.taa and plan.exposure and state.taa_valid and state.exposure_valid
+    image = renderer.display_image()
+    bgra = runner.host("display").reshape(h, w, 4)
+    np.testing.assert_array_equal(image, bgra[..., [2, 1, 0, 3]])
+    np.testing.assert_array_equal(renderer.download("display.hdr", np.uint16)[:w * h * 4],
+                                  runner.host(runner.displayed()))
+    np.testing.assert_array_equal(renderer.download("exposure", np.uint32)[:1], runner.host("exposure"))

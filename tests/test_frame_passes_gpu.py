@@ -21,6 +21,9 @@ CASES = {
     # Every ray through the BVH, 4 GI candidates.
     "bvh-rays": dict(scene=(rb.SCENE_CORNELL, 0, 0), size=(64, 64), frames=2,
                      overrides=dict(gi_divisor=1, ray_mode=rb.RAY_BVH, initial_candidates=4)),
+    # The display chain with auto exposure and ACES (every other case runs TAA and AgX, the defaults).
+    "display-auto": dict(scene=(rb.SCENE_CORNELL, 0, 0), size=(96, 96), frames=4,
+                         overrides=dict(gi_divisor=1, auto_exposure=1, tonemapper=0)),
     # Depth buffer only, screen-space reuse, GI without DI, no denoiser.
     "screen-space": dict(scene=(rb.SCENE_COURTYARD, 0, 20000), size=(128, 72), frames=3,
                          overrides=dict(ray_mode=rb.RAY_SCREEN, world_space_reuse=0, direct_lighting=1, denoiser=0)),
@@ -52,6 +55,9 @@ def test_frame_passes_bit_exact(case):
     assert np.count_nonzero(hdr[:, :3]) > 0.2 * hdr[:, :3].size
     gi = oracle_run.host("gi.color1" if oracle_run.history_read == 1 else "gi.color0")
     assert np.count_nonzero(gi) > 0
+    # The display chain ran: TAA blended a history, the image is tone-mapped.
+    assert oracle_run.display_taa and oracle_run.state.taa_valid
+    assert np.count_nonzero(oracle_run.host("display")) > 0
 
 
 @pytest.mark.gpu
