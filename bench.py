@@ -69,6 +69,9 @@ PASS_PIXEL_BYTES = {
     # radiance-cache training: per training sample a query and a target (80 B) and the hash-grid
     # gather of two queries (2 x 512 B); counted per GI pixel only when it runs
     "cache": ("none", 0),
+    # TAA + tone mapping, fused: the composite (3x3 neighbourhood, read once), depth, the TAA history,
+    # the TAA target and the BGRA8 display (8 + 4 + 8 + 8 + 4); the exposure's 4,096 samples are noise
+    "display": ("full", 32),
 }
 
 
@@ -189,7 +192,7 @@ def reference_arm(args, rank: int, world: int) -> None:
         "impl": "reference", "metric": METRIC, "value": value, "unit": "ms/frame", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"1920x1080 frame, seeded 1M-triangle city scene, GI 1/2 res + DI + SVGF x5",
+        "config": {"workload": f"1920x1080 frame, seeded 1M-triangle city scene, GI 1/2 res + DI + SVGF x5 + TAA + AgX tone mapping",
                    "scene_triangles": TRIANGLES, "width": WIDTH, "height": HEIGHT},
         "cpu_baseline": {"value": value, "unit": "ms/frame", "cores": baseline["cores"], "kind": "port",
                          "sample": baseline["sample"]},
@@ -465,17 +468,19 @@ def own_arm(args, rank: int, world: int) -> None:
     peak, peak_kind = load_peaks()
     achieved = float(pass_bytes[passes[dominant]] / (mean_pass[dominant] * 1e-3) / 1e9) if mean_pass[dominant] > 0 else 0.0
     share = {name: (mean_pass[i] / ms_per_frame if ms_per_frame > 0 else 0.0) for i, name in enumerate(passes)}
-    # shadow, G-buffer, DI x2, grid x2, GI temporal (3 kernels as a wavefront), GI spatial, denoiser, composite
+    # shadow, G-buffer, DI x2, grid x2, GI temporal (3 kernels as a wavefront), GI spatial, denoiser, composite,
+    # display (auto exposure when on, then TAA + tone mapping)
     gi_temporal_kernels = 3 if settings.wavefront else 1
     launches = (2 + (2 if plan.di_active else 0) + 2 + gi_temporal_kernels + 1
-                + (1 + plan.atrous_iterations if plan.denoiser else 0) + 1)
+                + (1 + plan.atrous_iterations if plan.denoiser else 0) + 1
+                + ((1 + plan.exposure) if plan.display else 0))
 
     baseline = cpu_baseline(steps=1, scale=2) if not args.no_cpu_baseline else None
     line = {
         "metric": METRIC, "value": ms_per_frame, "unit": "ms/frame", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_frame, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
-        "config": {"workload": "1920x1080 frame, seeded 1M-triangle city scene, GI 1/2 res + DI + SVGF x5",
+        "config": {"workload": "1920x1080 frame, seeded 1M-triangle city scene, GI 1/2 res + DI + SVGF x5 + TAA + AgX tone mapping",
                    "scene_triangles": mesh.triangle_count, "width": WIDTH, "height": HEIGHT,
                    "gi_resolution": [params.gi_width, params.gi_height], "di_lights": params.di_light_count,
                    "grid_table_size": params.grid_table_size, "graph": bool(args.graph),
