@@ -77,6 +77,8 @@ typedef struct RestirSettings
 	float adaptation_speed;  /* settings.h:215, per second */
 	int display;             /* no reference counterpart (the reference always draws to its
 	                            window): 0 skips exposure, TAA and tone mapping */
+	int bvh_on_device;       /* no reference counterpart: 1 builds the scene's BVH on the GPU
+	                            (restir_bvh_build_gpu, the same buffer), 0 on the host */
 } RestirSettings;
 
 /* FrameInput (renderer.h) with the fly camera's pose. */

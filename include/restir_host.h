@@ -77,6 +77,12 @@ typedef struct RestirBvhDesc
 } RestirBvhDesc;
 
 void* restir_bvh_build(const RestirMeshDesc* mesh, int threads);
+/* The same BVH built on the current CUDA device (binned SAH breadth first,
+ * std::partition's permutation reproduced in parallel): the buffer, order,
+ * normals and emitters equal restir_bvh_build's bit for bit. stream: a
+ * cudaStream_t (null: the default stream); waits for it. No counterpart in
+ * the reference (its builder runs on the host, bvh.cpp:253). */
+void* restir_bvh_build_gpu(const RestirMeshDesc* mesh, void* stream);
 int restir_bvh_describe(void* bvh, RestirBvhDesc* out);
 void restir_bvh_destroy(void* bvh);
 

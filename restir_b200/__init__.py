@@ -83,6 +83,7 @@ _SIGNATURES = {
     "restir_renderer_profile_frame": (C.c_int, [P, C.POINTER(RestirFrameInput), P]),
     "restir_renderer_pass_history": (C.c_int, [P, u32, P]),
     # restir_host.h
+    "restir_bvh_build_gpu": (P, [C.POINTER(RestirMeshDesc), P]),
     "restir_mesh_procedural": (P, [C.c_int, u32, u32]),
     "restir_mesh_create": (P, [C.POINTER(RestirMeshDesc)]),
     "restir_mesh_describe": (C.c_int, [P, C.POINTER(RestirMeshDesc)]),
@@ -213,6 +214,26 @@ class Mesh:
     def procedural(cls, kind: int, seed: int = 0, triangles: int = 0) -> "Mesh":
         return cls(load().restir_mesh_procedural(kind, seed, triangles))
 
+    @classmethod
+    def from_arrays(cls, positions: np.ndarray, triangle_material: np.ndarray, materials: np.ndarray,
+                    normals: np.ndarray | None = None) -> "Mesh":
+        """A mesh from host arrays (copied): 9 floats per triangle, a material index per
+        triangle, 8 floats per material (base rgb, roughness, emission rgb, metallic);
+        normals (3 per triangle) default to the geometric ones."""
+        positions = np.ascontiguousarray(positions, np.float32).reshape(-1)
+        triangle_material = np.ascontiguousarray(triangle_material, np.uint32).reshape(-1)
+        materials = np.ascontiguousarray(materials, np.float32).reshape(-1)
+        d = RestirMeshDesc()
+        d.triangle_count = len(triangle_material)
+        d.positions = positions.ctypes.data
+        if normals is not None:
+            normals = np.ascontiguousarray(normals, np.float32).reshape(-1)
+            d.normals = normals.ctypes.data
+        d.triangle_material = triangle_material.ctypes.data
+        d.material_count = len(materials) // 8
+        d.materials = materials.ctypes.data
+        return cls(load().restir_mesh_create(C.byref(d)))
+
     @property
     def triangle_count(self) -> int:
         return self.desc.triangle_count
@@ -228,13 +249,17 @@ class Mesh:
 
 
 class Bvh:
-    """The reference layout (src/bvh.h) built by this library's host builder."""
+    """The reference layout (src/bvh.h) built by this library's host builder,
+    or on the GPU (device=True: restir_bvh_build_gpu, the same buffer)."""
 
-    def __init__(self, mesh: Mesh, threads: int = 0):
-        threads = threads or (os.cpu_count() or 1)
-        self.handle = load().restir_bvh_build(C.byref(mesh.desc), threads)
+    def __init__(self, mesh: Mesh, threads: int = 0, device: bool = False):
+        if device:
+            self.handle = load().restir_bvh_build_gpu(C.byref(mesh.desc), None)
+        else:
+            threads = threads or (os.cpu_count() or 1)
+            self.handle = load().restir_bvh_build(C.byref(mesh.desc), threads)
         if not self.handle:
-            raise RuntimeError("restir_bvh_build failed")
+            raise RuntimeError("restir_bvh_build_gpu failed" if device else "restir_bvh_build failed")
         self.desc = RestirBvhDesc()
         check(load().restir_bvh_describe(self.handle, C.byref(self.desc)), "restir_bvh_describe")
         d = self.desc

@@ -106,7 +106,7 @@ class RestirSettings(C.Structure):
         ("wavefront", C.c_uint32), ("radiance_cache", C.c_uint32), ("cache_training_samples", C.c_uint32),
         ("wave_visibility", C.c_uint32),
         ("taa", C.c_int), ("auto_exposure", C.c_int), ("tonemapper", C.c_int), ("exposure_ev", C.c_float),
-        ("adaptation_speed", C.c_float), ("display", C.c_int),
+        ("adaptation_speed", C.c_float), ("display", C.c_int), ("bvh_on_device", C.c_int),
     ]
 
 

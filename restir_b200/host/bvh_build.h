@@ -35,6 +35,10 @@ struct BvhResult
 
 BvhResult buildBvh(const Mesh& mesh, int threads);
 
+// The same BVH built on the current CUDA device (csrc/bvh_build.cu), on a
+// cudaStream_t; waits for it. Returns a RESTIR_* status.
+int buildBvhGpu(const Mesh& mesh, void* stream, BvhResult& result);
+
 struct LightListResult
 {
 	std::vector<float> data; // 16 floats per light

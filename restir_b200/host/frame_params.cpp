@@ -93,6 +93,7 @@ extern "C" void restir_settings_default(RestirSettings* s)
 	s->exposure_ev = 0.0f;
 	s->adaptation_speed = 1.5f;
 	s->display = 1;
+	s->bvh_on_device = 1;
 }
 
 extern "C" int restir_frame_params(const RestirSettings* requested, const RestirMeshDesc* scene, uint32_t light_count,

@@ -1,4 +1,5 @@
 // C ABI of include/restir_host.h over the host scene code.
+#include "../../include/restir_gpu.h"
 #include "bvh_build.h"
 
 #include <cmath>
@@ -150,6 +151,36 @@ extern "C" void* restir_bvh_build(const RestirMeshDesc* desc, int threads)
 	if (handle != nullptr)
 	{
 		handle->bvh = buildBvh(*static_cast<Mesh*>(meshHandle), threads);
+		for (const Emitter& e : handle->bvh.emitters)
+		{
+			handle->bvh.emitterFloats.push_back(float(e.triangle));
+			handle->bvh.emitterFloats.insert(handle->bvh.emitterFloats.end(), e.vertices, e.vertices + 9);
+			handle->bvh.emitterFloats.insert(handle->bvh.emitterFloats.end(), e.emission, e.emission + 3);
+		}
+	}
+	restir_mesh_destroy(meshHandle);
+	return handle;
+}
+
+extern "C" void* restir_bvh_build_gpu(const RestirMeshDesc* desc, void* stream)
+{
+	if (desc == nullptr)
+	{
+		return nullptr;
+	}
+	void* meshHandle = restir_mesh_create(desc);
+	if (meshHandle == nullptr)
+	{
+		return nullptr;
+	}
+	BvhHandle* handle = new (std::nothrow) BvhHandle();
+	if (handle != nullptr && buildBvhGpu(*static_cast<Mesh*>(meshHandle), stream, handle->bvh) != RESTIR_OK)
+	{
+		delete handle;
+		handle = nullptr;
+	}
+	if (handle != nullptr)
+	{
 		for (const Emitter& e : handle->bvh.emitters)
 		{
 			handle->bvh.emitterFloats.push_back(float(e.triangle));

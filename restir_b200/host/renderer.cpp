@@ -118,8 +118,20 @@ public:
 			std::memcpy(m_settings.light_position, mesh.lightPosition, sizeof(m_settings.light_position));
 			m_settings.sky_enabled = mesh.sky ? 1 : 0;
 		}
-		m_scene->bvh = buildBvh(mesh, 8);
-		int status = upload(m_scene->buffers["bvh"], m_scene->bvh.data.data(), m_scene->bvh.data.size() * sizeof(float));
+		int status = 0;
+		if (m_settings.bvh_on_device)
+		{
+			if (buildBvhGpu(mesh, m_stream, m_scene->bvh) != RESTIR_OK)
+			{
+				m_scene->has = false;
+				return RESTIR_ERROR_LAUNCH;
+			}
+		}
+		else
+		{
+			m_scene->bvh = buildBvh(mesh, 8);
+		}
+		status |= upload(m_scene->buffers["bvh"], m_scene->bvh.data.data(), m_scene->bvh.data.size() * sizeof(float));
 		status |= upload(m_scene->buffers["normals"], m_scene->bvh.triangleNormals.data(), m_scene->bvh.triangleNormals.size() * sizeof(float));
 		status |= upload(m_scene->buffers["materials"], mesh.materialData.data(), mesh.materialData.size() * sizeof(float));
 		m_scene->lightsKey.clear();
