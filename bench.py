@@ -250,6 +250,29 @@ def cache_kernels(args) -> None:
                       "status": rb.status_flags()}), flush=True)
 
 
+def bvh_build(args) -> None:
+    """--bvh-build: scene preparation, the BVH of the seeded city scene at 1M and
+    4M triangles (the stress configuration's size) built on the device
+    (restir_bvh_build_gpu) and on the host (16 threads), with a check that the
+    two buffers are identical."""
+    import restir_b200 as rb
+    lines = {}
+    for triangles in (TRIANGLES, 4 * TRIANGLES):
+        mesh = rb.Mesh.procedural(rb.SCENE_CITY, 0, triangles)
+        device_ms = []
+        for step in range(args.warmup + args.steps):
+            bvh = rb.Bvh(mesh, device=True)
+            if step >= args.warmup:
+                device_ms.append(bvh.desc.build_ms)
+        host = rb.Bvh(mesh)
+        identical = bool(np.array_equal(bvh.data.view(np.uint32), host.data.view(np.uint32))
+                         and np.array_equal(bvh.order, host.order))
+        lines[str(mesh.triangle_count)] = {"device_ms": float(np.median(device_ms)), "host_ms": host.desc.build_ms,
+                                           "host_threads": os.cpu_count(), "nodes": int(host.desc.node_count),
+                                           "identical": identical}
+    print(json.dumps({"bvh_build": lines, "steps": args.steps, "warmup": args.warmup}), flush=True)
+
+
 BATCH_SIZES = [(640, 360), (960, 540), (1280, 720), (1920, 1080), (800, 450), (1600, 900), (1024, 576), (1440, 810)]
 
 
@@ -531,6 +554,8 @@ def main():
                         help="the batched multi-view form (8 views of uneven resolution in one frame)")
     parser.add_argument("--cache-kernels", action="store_true",
                         help="time the radiance cache's query and training kernels alone (profiling)")
+    parser.add_argument("--bvh-build", action="store_true",
+                        help="time the device BVH builder against the host builder (1M and 4M triangles)")
     parser.add_argument("--quick", action="store_true",
                         help="profiling runs: W + K frames of the workload, no reference, no report")
     args = parser.parse_args()
@@ -539,6 +564,8 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus if args.gpus == 1 else 1)))
     if args.cache_kernels:
         cache_kernels(args)
+    elif args.bvh_build:
+        bvh_build(args)
     elif args.batched:
         batched(args)
     elif args.impl == "reference":

@@ -817,23 +817,44 @@ __global__ void triangleRowsKernel(const uint32_t* __restrict__ order, uint32_t 
 	emissive[slot] = (mat[4] > 0.0f || mat[5] > 0.0f || mat[6] > 0.0f) ? 1u : 0u;
 }
 
+// The BVH slots of the emissive triangles, in slot order, with their mesh triangles.
+__global__ void emitterListKernel(const uint32_t* __restrict__ emissive, const uint32_t* __restrict__ offsets,
+	const uint32_t* __restrict__ order, uint32_t n, uint2* list)
+{
+	const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+	if (slot < n && emissive[slot] != 0u)
+	{
+		list[offsets[slot]] = make_uint2(slot, order[slot]);
+	}
+}
+
+__global__ void identityKernel(uint32_t* order, uint32_t n)
+{
+	const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t < n)
+	{
+		order[t] = t;
+	}
+}
+
 // --- host side ----------------------------------------------------------------------------
 
+// Temporary device memory from the stream-ordered pool, freed on the stream.
 template<typename T>
 struct DeviceArray
 {
 	T* p = nullptr;
-	size_t count = 0;
-	cudaError_t allocate(size_t n)
+	cudaStream_t stream = nullptr;
+	bool allocate(size_t n, cudaStream_t s)
 	{
-		count = n;
-		return cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T));
+		stream = s;
+		return cudaMallocAsync(reinterpret_cast<void**>(&p), std::max<size_t>(n, 1) * sizeof(T), s) == cudaSuccess;
 	}
 	~DeviceArray()
 	{
 		if (p != nullptr)
 		{
-			cudaFree(p);
+			cudaFreeAsync(p, stream);
 		}
 	}
 };
@@ -845,7 +866,7 @@ uint32_t blocksFor(uint64_t n, uint32_t threads)
 
 } // namespace
 
-int buildBvhGpu(const Mesh& mesh, void* streamHandle, BvhResult& result)
+int buildBvhGpu(const Mesh& mesh, void* streamHandle, BvhResult& result, DeviceBvh* device)
 {
 	const cudaStream_t stream = static_cast<cudaStream_t>(streamHandle);
 	const auto start = std::chrono::steady_clock::now();
@@ -869,41 +890,51 @@ int buildBvhGpu(const Mesh& mesh, void* streamHandle, BvhResult& result)
 		}
 	}
 	const uint32_t maxNodes = 2 * n;
+	const uint32_t maxTasks = n / kSmallTask + 1;
 	DeviceArray<float> positions, normals, materials, soup;
 	DeviceArray<uint32_t> material, order, flags, prefix, leftPos, rightPos, small, bins, chunks, chunkStart, rootWords,
-		size, index, emissive;
-	DeviceArray<uint8_t> twoSided;
+		size, index, emissive, emitterOffsets;
+	DeviceArray<uint2> emitterList;
+	DeviceArray<uint8_t> twoSided, scanScratch;
 	DeviceArray<TreeNode> nodes;
 	DeviceArray<Task> tasks[2];
 	DeviceArray<Counters> counters;
-	DeviceArray<float4> rows, triangleNormals;
-	bool ok = positions.allocate(size_t(n) * 9) == cudaSuccess && normals.allocate(size_t(n) * 3) == cudaSuccess
-		&& materials.allocate(mesh.materialData.size()) == cudaSuccess && soup.allocate(size_t(n) * 9) == cudaSuccess
-		&& material.allocate(n) == cudaSuccess && order.allocate(n) == cudaSuccess && flags.allocate(n + 1) == cudaSuccess
-		&& prefix.allocate(n + 1) == cudaSuccess && leftPos.allocate(n) == cudaSuccess && rightPos.allocate(n) == cudaSuccess
-		&& small.allocate(n) == cudaSuccess && nodes.allocate(maxNodes) == cudaSuccess && tasks[0].allocate(n / kSmallTask + 1) == cudaSuccess
-		&& tasks[1].allocate(n / kSmallTask + 1) == cudaSuccess && counters.allocate(1) == cudaSuccess
-		&& rootWords.allocate(12) == cudaSuccess && size.allocate(maxNodes) == cudaSuccess && index.allocate(maxNodes) == cudaSuccess
-		&& rows.allocate(2 * size_t(maxNodes) + 4 * size_t(n)) == cudaSuccess && triangleNormals.allocate(n) == cudaSuccess
-		&& emissive.allocate(n + 1) == cudaSuccess && chunks.allocate(n / kSmallTask + 2) == cudaSuccess
-		&& chunkStart.allocate(n / kSmallTask + 2) == cudaSuccess
-		&& bins.allocate(size_t(n / kSmallTask + 1) * kTaskBins) == cudaSuccess;
-	if (!mesh.twoSided.empty())
-	{
-		ok = ok && twoSided.allocate(n) == cudaSuccess;
-	}
-	if (!ok)
-	{
-		return RESTIR_ERROR_OUT_OF_MEMORY;
-	}
-	// Scan scratch (CUB), sized for the largest scan.
+	bool ok = positions.allocate(size_t(n) * 9, stream) && normals.allocate(size_t(n) * 3, stream)
+		&& materials.allocate(mesh.materialData.size(), stream) && soup.allocate(size_t(n) * 9, stream)
+		&& material.allocate(n, stream) && order.allocate(n, stream) && flags.allocate(n + 1, stream)
+		&& prefix.allocate(n + 1, stream) && leftPos.allocate(n, stream) && rightPos.allocate(n, stream)
+		&& small.allocate(n, stream) && nodes.allocate(maxNodes, stream) && tasks[0].allocate(maxTasks, stream)
+		&& tasks[1].allocate(maxTasks, stream) && counters.allocate(1, stream) && rootWords.allocate(12, stream)
+		&& size.allocate(maxNodes, stream) && index.allocate(maxNodes, stream) && emissive.allocate(n + 1, stream)
+		&& emitterOffsets.allocate(n + 1, stream) && emitterList.allocate(n, stream)
+		&& chunks.allocate(maxTasks + 1, stream) && chunkStart.allocate(maxTasks + 1, stream)
+		&& bins.allocate(size_t(maxTasks) * kTaskBins, stream)
+		&& (mesh.twoSided.empty() || twoSided.allocate(n, stream));
+	// The outputs: node and triangle rows, shading normals (kept on the device or downloaded).
+	float4* rows = nullptr;
+	float4* triangleNormals = nullptr;
+	ok = ok && cudaMalloc(&rows, (2 * size_t(maxNodes) + 4 * size_t(n)) * sizeof(float4)) == cudaSuccess;
+	ok = ok && cudaMalloc(&triangleNormals, size_t(n) * sizeof(float4)) == cudaSuccess;
 	size_t scanBytes = 0;
 	cub::DeviceScan::ExclusiveSum(nullptr, scanBytes, flags.p, prefix.p, n + 1, stream);
-	DeviceArray<uint8_t> scanScratch;
-	if (scanScratch.allocate(scanBytes) != cudaSuccess)
+	ok = ok && scanScratch.allocate(scanBytes, stream);
+	auto releaseOutputs = [&]()
 	{
+		cudaFree(rows);
+		cudaFree(triangleNormals);
+	};
+	if (!ok)
+	{
+		cudaStreamSynchronize(stream);
+		releaseOutputs();
 		return RESTIR_ERROR_OUT_OF_MEMORY;
 	}
+	auto fail = [&](int status)
+	{
+		cudaStreamSynchronize(stream);
+		releaseOutputs();
+		return status;
+	};
 	cudaMemcpyAsync(positions.p, mesh.positions.data(), size_t(n) * 9 * sizeof(float), cudaMemcpyHostToDevice, stream);
 	cudaMemcpyAsync(normals.p, mesh.normals.data(), size_t(n) * 3 * sizeof(float), cudaMemcpyHostToDevice, stream);
 	cudaMemcpyAsync(materials.p, mesh.materialData.data(), mesh.materialData.size() * sizeof(float), cudaMemcpyHostToDevice, stream);
@@ -912,12 +943,7 @@ int buildBvhGpu(const Mesh& mesh, void* streamHandle, BvhResult& result)
 	{
 		cudaMemcpyAsync(twoSided.p, mesh.twoSided.data(), n, cudaMemcpyHostToDevice, stream);
 	}
-	std::vector<uint32_t> identity(n);
-	for (uint32_t t = 0; t < n; ++t)
-	{
-		identity[t] = t;
-	}
-	cudaMemcpyAsync(order.p, identity.data(), size_t(n) * sizeof(uint32_t), cudaMemcpyHostToDevice, stream);
+	identityKernel<<<blocksFor(n, 256), 256, 0, stream>>>(order.p, n);
 	cudaMemsetAsync(counters.p, 0, sizeof(Counters), stream);
 	cudaMemsetAsync(flags.p, 0, (n + 1) * sizeof(uint32_t), stream);
 
@@ -933,6 +959,7 @@ int buildBvhGpu(const Mesh& mesh, void* streamHandle, BvhResult& result)
 			init[k] = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
 		}
 		cudaMemcpyAsync(rootWords.p, init, sizeof(init), cudaMemcpyHostToDevice, stream);
+		cudaStreamSynchronize(stream); // init lives on this stack frame
 	}
 	rootBoundsKernel<<<std::min<uint32_t>(blocksFor(n, 256), 1184), 256, 0, stream>>>(s, rootWords.p);
 	rootTaskKernel<<<1, 1, 0, stream>>>(rootWords.p, n, nodes.p, tasks[0].p, counters.p);
@@ -945,12 +972,14 @@ int buildBvhGpu(const Mesh& mesh, void* streamHandle, BvhResult& result)
 	}
 	else if (n > 1)
 	{
-		const uint32_t zero = 0;
-		cudaMemcpyAsync(small.p, &zero, sizeof(zero), cudaMemcpyHostToDevice, stream);
-		host.smallTasks = 1;
-		cudaMemcpyAsync(&counters.p->smallTasks, &host.smallTasks, sizeof(uint32_t), cudaMemcpyHostToDevice, stream);
+		// The root is a small subtree: node 0, one small task.
+		cudaMemsetAsync(small.p, 0, sizeof(uint32_t), stream);
+		const uint32_t one = 1;
+		cudaMemcpyAsync(&counters.p->smallTasks, &one, sizeof(uint32_t), cudaMemcpyHostToDevice, stream);
+		cudaStreamSynchronize(stream);
 	}
 	int current = 0;
+	uint32_t chunkTotal = 0;
 	while (taskCount > 0)
 	{
 		Task* level = tasks[current].p;
@@ -958,14 +987,13 @@ int buildBvhGpu(const Mesh& mesh, void* streamHandle, BvhResult& result)
 		chunkCountKernel<<<blocksFor(taskCount + 1, 256), 256, 0, stream>>>(level, taskCount, chunks.p);
 		size_t bytes = scanBytes;
 		cub::DeviceScan::ExclusiveSum(scanScratch.p, bytes, chunks.p, chunkStart.p, taskCount + 1, stream);
-		uint32_t chunkTotal = 0;
 		cudaMemcpyAsync(&chunkTotal, chunkStart.p + taskCount, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
 		binInitKernel<<<std::min<uint32_t>(blocksFor(size_t(taskCount) * kTaskBins, 256), 4096), 256, 0, stream>>>(
 			bins.p, taskCount * kTaskBins);
 		cudaMemsetAsync(&counters.p->nextTasks, 0, sizeof(uint32_t), stream);
 		if (cudaStreamSynchronize(stream) != cudaSuccess)
 		{
-			return RESTIR_ERROR_LAUNCH;
+			return fail(RESTIR_ERROR_LAUNCH);
 		}
 		binKernel<<<chunkTotal, 256, 0, stream>>>(level, taskCount, chunkStart.p, order.p, s, bins.p);
 		sahKernel<<<blocksFor(taskCount, 128), 128, 0, stream>>>(level, taskCount, bins.p, nodes.p, next, small.p, counters.p);
@@ -980,11 +1008,11 @@ int buildBvhGpu(const Mesh& mesh, void* streamHandle, BvhResult& result)
 		cudaMemcpyAsync(&host, counters.p, sizeof(Counters), cudaMemcpyDeviceToHost, stream);
 		if (cudaStreamSynchronize(stream) != cudaSuccess)
 		{
-			return RESTIR_ERROR_LAUNCH;
+			return fail(RESTIR_ERROR_LAUNCH);
 		}
 		if (host.errors != 0u)
 		{
-			return RESTIR_ERROR_LAUNCH;
+			return fail(RESTIR_ERROR_LAUNCH);
 		}
 		taskCount = host.nextTasks;
 		current = 1 - current;
@@ -992,7 +1020,7 @@ int buildBvhGpu(const Mesh& mesh, void* streamHandle, BvhResult& result)
 	cudaMemcpyAsync(&host, counters.p, sizeof(Counters), cudaMemcpyDeviceToHost, stream);
 	if (cudaStreamSynchronize(stream) != cudaSuccess)
 	{
-		return RESTIR_ERROR_LAUNCH;
+		return fail(RESTIR_ERROR_LAUNCH);
 	}
 	if (host.smallTasks > 0)
 	{
@@ -1002,7 +1030,7 @@ int buildBvhGpu(const Mesh& mesh, void* streamHandle, BvhResult& result)
 	cudaMemcpyAsync(&host, counters.p, sizeof(Counters), cudaMemcpyDeviceToHost, stream);
 	if (cudaStreamSynchronize(stream) != cudaSuccess)
 	{
-		return RESTIR_ERROR_LAUNCH;
+		return fail(RESTIR_ERROR_LAUNCH);
 	}
 	const uint32_t nodeCount = host.nodes;
 	const uint32_t depth = host.maxDepth;
@@ -1015,39 +1043,60 @@ int buildBvhGpu(const Mesh& mesh, void* streamHandle, BvhResult& result)
 	{
 		indexKernel<<<blocksFor(nodeCount, 256), 256, 0, stream>>>(nodes.p, nodeCount, d, size.p, index.p);
 	}
-	nodeRowsKernel<<<blocksFor(nodeCount, 256), 256, 0, stream>>>(nodes.p, nodeCount, size.p, index.p, rows.p);
+	nodeRowsKernel<<<blocksFor(nodeCount, 256), 256, 0, stream>>>(nodes.p, nodeCount, size.p, index.p, rows);
+	cudaMemsetAsync(emissive.p + n, 0, sizeof(uint32_t), stream);
 	triangleRowsKernel<<<blocksFor(n, 256), 256, 0, stream>>>(order.p, n, positions.p, normals.p, material.p,
-		mesh.twoSided.empty() ? nullptr : twoSided.p, materials.p, rows.p + 2 * size_t(nodeCount), triangleNormals.p,
+		mesh.twoSided.empty() ? nullptr : twoSided.p, materials.p, rows + 2 * size_t(nodeCount), triangleNormals,
 		emissive.p);
+	size_t bytes = scanBytes;
+	cub::DeviceScan::ExclusiveSum(scanScratch.p, bytes, emissive.p, emitterOffsets.p, n + 1, stream);
+	emitterListKernel<<<blocksFor(n, 256), 256, 0, stream>>>(emissive.p, emitterOffsets.p, order.p, n, emitterList.p);
+	uint32_t emitterCount = 0;
+	cudaMemcpyAsync(&emitterCount, emitterOffsets.p + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
+	if (cudaStreamSynchronize(stream) != cudaSuccess)
+	{
+		return fail(RESTIR_ERROR_LAUNCH);
+	}
+	std::vector<uint2> emitterPairs(emitterCount);
+	cudaMemcpyAsync(emitterPairs.data(), emitterList.p, size_t(emitterCount) * sizeof(uint2), cudaMemcpyDeviceToHost, stream);
 
 	result.nodeCount = nodeCount;
 	result.depth = depth;
 	result.triangleOffset = 2 * nodeCount;
-	result.data.resize((size_t(result.triangleOffset) + 4 * size_t(n)) * 4);
-	result.order.resize(n);
-	result.triangleNormals.resize(size_t(n) * 4);
-	std::vector<uint32_t> emissiveHost(n);
-	cudaMemcpyAsync(result.data.data(), rows.p, result.data.size() * sizeof(float), cudaMemcpyDeviceToHost, stream);
-	cudaMemcpyAsync(result.order.data(), order.p, size_t(n) * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
-	cudaMemcpyAsync(result.triangleNormals.data(), triangleNormals.p, result.triangleNormals.size() * sizeof(float),
-		cudaMemcpyDeviceToHost, stream);
-	cudaMemcpyAsync(emissiveHost.data(), emissive.p, size_t(n) * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
+	const size_t rowCount = size_t(result.triangleOffset) + 4 * size_t(n);
+	if (device == nullptr)
+	{
+		result.data.resize(rowCount * 4);
+		result.order.resize(n);
+		result.triangleNormals.resize(size_t(n) * 4);
+		cudaMemcpyAsync(result.data.data(), rows, rowCount * sizeof(float4), cudaMemcpyDeviceToHost, stream);
+		cudaMemcpyAsync(result.order.data(), order.p, size_t(n) * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
+		cudaMemcpyAsync(result.triangleNormals.data(), triangleNormals, size_t(n) * sizeof(float4), cudaMemcpyDeviceToHost,
+			stream);
+	}
 	if (cudaStreamSynchronize(stream) != cudaSuccess || cudaGetLastError() != cudaSuccess)
 	{
-		return RESTIR_ERROR_LAUNCH;
+		return fail(RESTIR_ERROR_LAUNCH);
 	}
-	for (uint32_t slot = 0; slot < n; ++slot)
+	for (const uint2& e : emitterPairs)
 	{
-		if (emissiveHost[slot] != 0u)
-		{
-			const uint32_t t = result.order[slot];
-			const Material& material = mesh.materials[mesh.material[t]];
-			Emitter e;
-			e.triangle = slot;
-			std::memcpy(e.vertices, &mesh.positions[size_t(t) * 9], sizeof(e.vertices));
-			std::memcpy(e.emission, material.emission, sizeof(e.emission));
-			result.emitters.push_back(e);
-		}
+		const Material& m = mesh.materials[mesh.material[e.y]];
+		Emitter emitter;
+		emitter.triangle = e.x;
+		std::memcpy(emitter.vertices, &mesh.positions[size_t(e.y) * 9], sizeof(emitter.vertices));
+		std::memcpy(emitter.emission, m.emission, sizeof(emitter.emission));
+		result.emitters.push_back(emitter);
+	}
+	if (device != nullptr)
+	{
+		device->rows = rows;
+		device->rowsBytes = rowCount * sizeof(float4);
+		device->normals = triangleNormals;
+		device->normalsBytes = size_t(n) * sizeof(float4);
+	}
+	else
+	{
+		releaseOutputs();
 	}
 	result.buildMs = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - start).count();
 	return RESTIR_OK;

@@ -35,9 +35,21 @@ struct BvhResult
 
 BvhResult buildBvh(const Mesh& mesh, int threads);
 
+// Device copies of a BVH's node and triangle rows and its shading normals
+// (cudaMalloc'd; the owner frees them with cudaFree).
+struct DeviceBvh
+{
+	void* rows = nullptr;
+	uint64_t rowsBytes = 0;
+	void* normals = nullptr;
+	uint64_t normalsBytes = 0;
+};
+
 // The same BVH built on the current CUDA device (csrc/bvh_build.cu), on a
-// cudaStream_t; waits for it. Returns a RESTIR_* status.
-int buildBvhGpu(const Mesh& mesh, void* stream, BvhResult& result);
+// cudaStream_t; waits for it. Returns a RESTIR_* status. With device null the
+// rows, order and normals are downloaded into result; otherwise they stay on
+// the device in *device and result carries the counts and emitters only.
+int buildBvhGpu(const Mesh& mesh, void* stream, BvhResult& result, DeviceBvh* device = nullptr);
 
 struct LightListResult
 {

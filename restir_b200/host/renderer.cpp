@@ -121,18 +121,24 @@ public:
 		int status = 0;
 		if (m_settings.bvh_on_device)
 		{
-			if (buildBvhGpu(mesh, m_stream, m_scene->bvh) != RESTIR_OK)
+			// Built on the device; the rows and normals stay there.
+			DeviceBvh device;
+			const int built = buildBvhGpu(mesh, m_stream, m_scene->bvh, &device);
+			if (built != RESTIR_OK)
 			{
 				m_scene->has = false;
-				return RESTIR_ERROR_LAUNCH;
+				return built;
 			}
+			m_scene->buffers["bvh"] = Buffer{ device.rows, device.rowsBytes };
+			m_scene->buffers["normals"] = Buffer{ device.normals, device.normalsBytes };
 		}
 		else
 		{
 			m_scene->bvh = buildBvh(mesh, 8);
+			status |= upload(m_scene->buffers["bvh"], m_scene->bvh.data.data(), m_scene->bvh.data.size() * sizeof(float));
+			status |= upload(m_scene->buffers["normals"], m_scene->bvh.triangleNormals.data(),
+				m_scene->bvh.triangleNormals.size() * sizeof(float));
 		}
-		status |= upload(m_scene->buffers["bvh"], m_scene->bvh.data.data(), m_scene->bvh.data.size() * sizeof(float));
-		status |= upload(m_scene->buffers["normals"], m_scene->bvh.triangleNormals.data(), m_scene->bvh.triangleNormals.size() * sizeof(float));
 		status |= upload(m_scene->buffers["materials"], mesh.materialData.data(), mesh.materialData.size() * sizeof(float));
 		m_scene->lightsKey.clear();
 		status |= updateLights();
