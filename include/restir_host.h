@@ -47,11 +47,22 @@ typedef struct RestirMeshDesc
 	float camera_yaw;
 	float camera_pitch;
 	int sky;                         /* whether the sky starts on */
+	const uint8_t* two_sided;        /* per triangle, 1 for double-sided materials; may be null */
 } RestirMeshDesc;
 
 void* restir_mesh_procedural(int kind, uint32_t seed, uint32_t target_triangles);
 /* A mesh from caller arrays (copied). */
 void* restir_mesh_create(const RestirMeshDesc* desc);
+/* A mesh from a glTF 2.0 file (.gltf with external or data-URI buffers, or
+ * .glb), as the reference's loadScene flattens a model (scene.cpp:105-381,
+ * 722-808): the default scene's nodes with their transforms, triangle-list
+ * primitives, triangles grouped by material in material order, material
+ * factors (base colour, metallic, roughness, emission times
+ * KHR_materials_emissive_strength, double-sided), the light placed by
+ * describeScene (scene.cpp:810-834) and the first view of main.cpp:58-83.
+ * Textures, vertex colours and sparse accessors are not read. Null on
+ * failure, with a message in error (may be null). */
+void* restir_mesh_load_gltf(const char* path, char* error, uint32_t error_capacity);
 int restir_mesh_describe(void* mesh, RestirMeshDesc* out);
 void restir_mesh_destroy(void* mesh);
 

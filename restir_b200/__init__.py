@@ -86,6 +86,7 @@ _SIGNATURES = {
     "restir_bvh_build_gpu": (P, [C.POINTER(RestirMeshDesc), P]),
     "restir_mesh_procedural": (P, [C.c_int, u32, u32]),
     "restir_mesh_create": (P, [C.POINTER(RestirMeshDesc)]),
+    "restir_mesh_load_gltf": (P, [C.c_char_p, C.c_char_p, u32]),
     "restir_mesh_describe": (C.c_int, [P, C.POINTER(RestirMeshDesc)]),
     "restir_mesh_destroy": (None, [P]),
     "restir_bvh_build": (P, [C.POINTER(RestirMeshDesc), C.c_int]),
@@ -213,6 +214,15 @@ class Mesh:
     @classmethod
     def procedural(cls, kind: int, seed: int = 0, triangles: int = 0) -> "Mesh":
         return cls(load().restir_mesh_procedural(kind, seed, triangles))
+
+    @classmethod
+    def load_gltf(cls, path) -> "Mesh":
+        """A mesh from a .gltf or .glb file (restir_mesh_load_gltf)."""
+        error = C.create_string_buffer(512)
+        handle = load().restir_mesh_load_gltf(str(path).encode(), error, len(error))
+        if not handle:
+            raise RuntimeError(f"restir_mesh_load_gltf: {error.value.decode(errors='replace')}")
+        return cls(handle)
 
     @classmethod
     def from_arrays(cls, positions: np.ndarray, triangle_material: np.ndarray, materials: np.ndarray,

@@ -72,7 +72,7 @@ class RestirMeshDesc(C.Structure):
         ("triangle_material", C.c_void_p), ("material_count", C.c_uint32), ("materials", C.c_void_p),
         ("bounds_min", f3), ("bounds_max", f3), ("center", f3), ("radius", C.c_float),
         ("light_position", f3), ("camera_eye", f3), ("camera_yaw", C.c_float), ("camera_pitch", C.c_float),
-        ("sky", C.c_int),
+        ("sky", C.c_int), ("two_sided", C.c_void_p),
     ]
 
 

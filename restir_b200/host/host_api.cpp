@@ -82,7 +82,14 @@ extern "C" void* restir_mesh_create(const RestirMeshDesc* desc)
 		}
 	}
 	mesh->material.assign(desc->triangle_material, desc->triangle_material + n);
-	mesh->twoSided.assign(n, 0);
+	if (desc->two_sided != nullptr)
+	{
+		mesh->twoSided.assign(desc->two_sided, desc->two_sided + n);
+	}
+	else
+	{
+		mesh->twoSided.assign(n, 0);
+	}
 	for (uint32_t m = 0; m < desc->material_count; ++m)
 	{
 		Material q;
@@ -128,6 +135,7 @@ extern "C" int restir_mesh_describe(void* handle, RestirMeshDesc* out)
 	out->camera_yaw = mesh->cameraYaw;
 	out->camera_pitch = mesh->cameraPitch;
 	out->sky = mesh->sky ? 1 : 0;
+	out->two_sided = mesh->twoSided.empty() ? nullptr : mesh->twoSided.data();
 	return 0;
 }
 
