@@ -72,6 +72,9 @@ PASS_PIXEL_BYTES = {
     # TAA + tone mapping, fused: the composite (3x3 neighbourhood, read once), depth, the TAA history,
     # the TAA target and the BGRA8 display (8 + 4 + 8 + 8 + 4); the exposure's 4,096 samples are noise
     "display": ("full", 32),
+    # indirect specular: G-buffer 12, history receiver and normal 32, specular history 8 and target 8,
+    # last frame's HDR at the hit 8
+    "specular": ("gi", 68),
 }
 
 
@@ -192,7 +195,7 @@ def reference_arm(args, rank: int, world: int) -> None:
         "impl": "reference", "metric": METRIC, "value": value, "unit": "ms/frame", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"1920x1080 frame, seeded 1M-triangle city scene, GI 1/2 res + DI + SVGF x5 + TAA + AgX tone mapping",
+        "config": {"workload": f"1920x1080 frame, seeded 1M-triangle city scene, GI 1/2 res + DI + specular GI + SVGF x5 + TAA + AgX tone mapping",
                    "scene_triangles": TRIANGLES, "width": WIDTH, "height": HEIGHT},
         "cpu_baseline": {"value": value, "unit": "ms/frame", "cores": baseline["cores"], "kind": "port",
                          "sample": baseline["sample"]},
@@ -496,14 +499,14 @@ def own_arm(args, rank: int, world: int) -> None:
     gi_temporal_kernels = 3 if settings.wavefront else 1
     launches = (2 + (2 if plan.di_active else 0) + 2 + gi_temporal_kernels + 1
                 + (1 + plan.atrous_iterations if plan.denoiser else 0) + 1
-                + ((1 + plan.exposure) if plan.display else 0))
+                + ((1 + plan.exposure) if plan.display else 0) + (1 if plan.specular else 0))
 
     baseline = cpu_baseline(steps=1, scale=2) if not args.no_cpu_baseline else None
     line = {
         "metric": METRIC, "value": ms_per_frame, "unit": "ms/frame", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_frame, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
-        "config": {"workload": "1920x1080 frame, seeded 1M-triangle city scene, GI 1/2 res + DI + SVGF x5 + TAA + AgX tone mapping",
+        "config": {"workload": "1920x1080 frame, seeded 1M-triangle city scene, GI 1/2 res + DI + specular GI + SVGF x5 + TAA + AgX tone mapping",
                    "scene_triangles": mesh.triangle_count, "width": WIDTH, "height": HEIGHT,
                    "gi_resolution": [params.gi_width, params.gi_height], "di_lights": params.di_light_count,
                    "grid_table_size": params.grid_table_size, "graph": bool(args.graph),

@@ -6,10 +6,9 @@
  * and runs the passes in the reference's order on one CUDA stream
  * (optionally replayed from a CUDA graph).
  *
- * Scope: the passes named in restir_gpu.h and the display chain of
- * restir_display.h (auto exposure, TAA, tone mapping into a BGRA8 image).
- * Specular GI and the debug views are not part of this driver; their
- * settings are fixed off.
+ * Scope: the passes named in restir_gpu.h (specular GI included) and the
+ * display chain of restir_display.h (auto exposure, TAA, tone mapping into a
+ * BGRA8 image). The debug views are not part of this driver.
  */
 #ifndef RESTIR_FRAME_H
 #define RESTIR_FRAME_H
@@ -79,6 +78,7 @@ typedef struct RestirSettings
 	                            window): 0 skips exposure, TAA and tone mapping */
 	int bvh_on_device;       /* no reference counterpart: 1 builds the scene's BVH on the GPU
 	                            (restir_bvh_build_gpu, the same buffer), 0 on the host */
+	int specular_gi;         /* indirect specular (glossy reflections, settings.h:195) */
 } RestirSettings;
 
 /* FrameInput (renderer.h) with the fly camera's pose. */
@@ -117,6 +117,7 @@ typedef struct RestirFramePlan
 	int display;                  /* the display chain runs (settings.display) */
 	int taa;                      /* TAA runs: settings.taa, not while the reference accumulates */
 	int exposure;                 /* auto exposure runs */
+	int specular;                 /* restir_gi_specular runs and the composite adds it */
 	float unjittered_view_proj[16]; /* this frame's, for the next frame's TAA */
 } RestirFramePlan;
 
@@ -149,7 +150,8 @@ void restir_frame_advance(const RestirParams* params, const RestirFramePlan* pla
 #define RESTIR_PASS_REFERENCE 9
 #define RESTIR_PASS_CACHE 10      /* radiance-cache training (no reference counterpart) */
 #define RESTIR_PASS_DISPLAY 11    /* auto exposure, TAA and tone mapping */
-#define RESTIR_PASS_COUNT 12
+#define RESTIR_PASS_SPECULAR 12   /* indirect specular (fs_specular.sc) */
+#define RESTIR_PASS_COUNT 13
 
 typedef struct RestirMetrics
 {

@@ -147,7 +147,9 @@ typedef struct RestirParams
 	 * bvh.sh:177-212, the reference's Vulkan build) instead of per lane
 	 * (traceBvhStackless); the hits are the same. */
 	float wave_visibility;
-	float pad_params[1];
+	/* u_compositeSpecular.x (renderer.cpp:955-961): the weight of the indirect
+	 * specular in restir_composite_specular (1 with specular GI on). */
+	float composite_specular;
 } RestirParams;
 
 /* Scene buffers, uploaded once per scene (renderer.cpp:365-419, 1170-1207). */
@@ -319,6 +321,30 @@ int restir_svgf_atrous(const RestirParams* params, int step, const uint16_t* inp
  * GI resolution. di_diffuse, di_specular may be null (black). */
 int restir_composite(const RestirParams* params, const RestirGBuffer* gbuffer, const float* shadow_atlas,
 	const uint16_t* gi, const uint16_t* di_diffuse, const uint16_t* di_specular, uint16_t* hdr, void* stream);
+
+/* The composite with indirect specular (fs_composite.sc:48-143 whole):
+ * restir_composite plus the GI-resolution specular target of
+ * restir_gi_specular, upsampled with the same weights as the diffuse GI and
+ * multiplied back by the split-sum specular albedo, the occlusion and
+ * params->composite_specular. specular may be null (then equal to
+ * restir_composite). */
+int restir_composite_specular(const RestirParams* params, const RestirGBuffer* gbuffer, const float* shadow_atlas,
+	const uint16_t* gi, const uint16_t* di_diffuse, const uint16_t* di_specular, const uint16_t* specular, uint16_t* hdr,
+	void* stream);
+
+/* Indirect specular (fs_specular.sc, renderer.cpp:835-855), at GI
+ * resolution: one GGX visible-normal ray per pixel, traced through the depth
+ * buffer then the BVH (the stackless walk of a fragment shader) then the sky;
+ * the radiance at a visible hit from last frame's HDR image (previous_hdr),
+ * else from the hit's direct, bounce and emitted light; demodulated by the
+ * specular albedo, clamped, and blended into the reprojected history
+ * (specular_history, same surface only) over 4 to 32 frames by roughness.
+ * Output RGBA16F: rgb demodulated radiance, a history length. The history is
+ * last frame's GI targets (receiver, normal, colour). specular must not
+ * alias specular_history. */
+int restir_gi_specular(const RestirParams* params, const RestirScene* scene, const RestirGBuffer* gbuffer,
+	const RestirGiHistory* history, const float* shadow_atlas, const uint16_t* surface_light, const uint16_t* previous_hdr,
+	const uint16_t* specular_history, uint16_t* specular, void* stream);
 
 /* The running mean of the composite in FP64 (fs_reference.sc):
  * mean = mean * (1 - w) + color * w with w = 1 / (frames + 1), NaN colours

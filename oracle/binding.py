@@ -43,6 +43,8 @@ _SIGNATURES = {
     "oracle_svgf_variance": (C.c_int, [PP, P, P, P, P, P]),
     "oracle_svgf_atrous": (C.c_int, [PP, C.c_int, P, P, P, P]),
     "oracle_composite": (C.c_int, [PP, PG, P, P, P, P, P]),
+    "oracle_composite_specular": (C.c_int, [PP, PG, P, P, P, P, P, P]),
+    "oracle_gi_specular": (C.c_int, [PP, PS, PG, C.POINTER(RestirGiHistory), P, P, P, P, P]),
     "oracle_reference_accumulate": (C.c_int, [PP, P, P, P, u32]),
     "oracle_error": (C.c_int, [PP, P, P, P, P]),
     "oracle_exposure": (C.c_int, [C.POINTER(RestirDisplayParams), P, P]),

@@ -41,6 +41,7 @@ LAYOUT = {
     "hdr": (np.uint16, 4, "full"),
     "ref.mean": (np.float64, 3, "full"), "ref.alpha": (np.uint8, 1, "full"),
     "taa0": (np.uint16, 4, "full"), "taa1": (np.uint16, 4, "full"), "display": (np.uint8, 4, "full"),
+    "specular0": (np.uint16, 4, "gi"), "specular1": (np.uint16, 4, "gi"),
     "exposure": (np.uint32, 1, "one"),
 }
 
@@ -59,6 +60,7 @@ class FrameRunner:
         self.history_read = 0
         self.di_read = 0
         self.taa_read = 0
+        self.specular_read = 0
         self.display_taa = False
         self.params = None
         self.plan = None
@@ -171,6 +173,12 @@ class FrameRunner:
             out.append(("gi_spatial", lambda: self.call("gi_spatial", P, self.scene, gb, current,
                                                         self.b(f"grid{hw}"), history, self.b("atlas"), surface,
                                                         self.b(f"gi.color{hw}"), self.b(f"gi.moments{hw}"))))
+        specular_write = f"specular{1 - self.specular_read}"
+        if plan.specular:
+            # Indirect specular (renderer.cpp:835-855): last frame's composite and specular history.
+            out.append(("gi_specular", lambda: self.call(
+                "gi_specular", P, self.scene, gb, history, self.b("atlas"), surface, self.b("hdr"),
+                self.b(f"specular{self.specular_read}"), self.b(specular_write))))
         denoised = f"gi.color{hw}"
         if plan.denoiser:
             out.append(("svgf_variance", lambda: self.call("svgf_variance", P, self.b(f"gi.color{hw}"),
@@ -185,8 +193,9 @@ class FrameRunner:
                     self.b(d)))))
         di_d = self.b("di.diffuse") if plan.di_active else self.b("black")
         di_s = self.b("di.specular") if plan.di_active else self.b("black")
-        out.append(("composite", lambda: self.call("composite", P, gb, self.b("atlas"), self.b(denoised), di_d, di_s,
-                                                   self.b("hdr"))))
+        spec = self.b(specular_write) if plan.specular else None
+        out.append(("composite", lambda: self.call("composite_specular", P, gb, self.b("atlas"), self.b(denoised), di_d,
+                                                   di_s, spec, self.b("hdr"))))
         if plan.reference_accumulate:
             out.append(("reference_accumulate", lambda: self.call(
                 "reference_accumulate", P, self.b("hdr"), self.b("ref.mean"), self.b("ref.alpha"),
@@ -259,6 +268,8 @@ class FrameRunner:
         rb.advance(self.params, self.plan, self.frame_input, self.state)
         self.history_read = 1 - self.history_read
         self.display_taa = bool(self.plan.display and self.plan.taa)
+        if self.plan.specular:
+            self.specular_read = 1 - self.specular_read
         if self.display_taa:
             self.taa_read = 1 - self.taa_read
         if self.plan.di_active:

@@ -1445,9 +1445,33 @@ parallelFor(int64_t(h), 8, [&](int64_t py_, int)
 
 /* --- composite (fs_composite.sc), reference, error ----------------------- */
 
+/* brdf.sh:68-76 */
+vec3 specularAlbedo(vec3 _f0, float _roughness, float _normalView)
+{
+	const vec4 c0(-1.0f, -0.0275f, -0.572f, 0.022f);
+	const vec4 c1(1.0f, 0.0425f, 1.04f, -0.04f);
+	const vec4 r(c0.x * _roughness + c1.x, c0.y * _roughness + c1.y, c0.z * _roughness + c1.z, c0.w * _roughness + c1.w);
+	const float a004 = min(r.x * r.x, rn_exp2(-9.28f * _normalView)) * r.x + r.y;
+	const vec2 scaleBias(-1.04f * a004 + r.z, 1.04f * a004 + r.w);
+	return _f0 * scaleBias.x + scaleBias.y;
+}
+
+extern "C" int oracle_composite_specular(const RestirParams* P, const RestirGBuffer* gb, const float* shadow_atlas,
+	const uint16_t* gi, const uint16_t* di_diffuse, const uint16_t* di_specular, const uint16_t* specular_target,
+	uint16_t* hdr);
+
 extern "C" int oracle_composite(const RestirParams* P, const RestirGBuffer* gb, const float* shadow_atlas,
 	const uint16_t* gi, const uint16_t* di_diffuse, const uint16_t* di_specular, uint16_t* hdr)
 {
+	return oracle_composite_specular(P, gb, shadow_atlas, gi, di_diffuse, di_specular, nullptr, hdr);
+}
+
+/* fs_composite.sc:48-143; the indirect specular term when specular_target is given. */
+extern "C" int oracle_composite_specular(const RestirParams* P, const RestirGBuffer* gb, const float* shadow_atlas,
+	const uint16_t* gi, const uint16_t* di_diffuse, const uint16_t* di_specular, const uint16_t* specular_target,
+	uint16_t* hdr)
+{
+	TexH4 specularTex = { specular_target, int(P->gi_width), int(P->gi_height) };
 	const int W = int(P->width), H = int(P->height);
 	const int w = int(P->gi_width), h = int(P->gi_height);
 	Screen screen;
@@ -1512,6 +1536,7 @@ parallelFor(int64_t(H), 8, [&](int64_t py_, int)
 			vec2 baseCoord = floor(texelCoord);
 			vec2 blend = texelCoord - baseCoord;
 			vec3 sum = vec3_splat(0.0f);
+			vec3 specularSum = vec3_splat(0.0f);
 			float weightSum = 0.0f;
 			for (int tapIndex = 0; tapIndex < 4; ++tapIndex)
 			{
@@ -1529,11 +1554,23 @@ parallelFor(int64_t(H), 8, [&](int64_t py_, int)
 					* step(abs(dot(tapPosition - position, surfaceNormal)), 0.03f * s)
 					* step(0.9f, dot(tapNormal, surfaceNormal));
 				sum += giTex.sample(tapUv).xyz() * weight;
+				if (specular_target != nullptr)
+				{
+					specularSum += specularTex.sample(tapUv).xyz() * weight;
+				}
 				weightSum += weight;
 			}
 			vec3 irradiance = weightSum > 0.0f ? sum / weightSum : giTex.sample(v_texcoord0).xyz();
 			vec3 indirect = irradiance
 				* (options[2] > 0.5f ? albedo * (1.0f - metallic) * emissiveOcclusion.w : vec3_splat(1.0f));
+			if (specular_target != nullptr)
+			{
+				/* fs_composite.sc:131-136 */
+				vec3 specularRadiance = weightSum > 0.0f ? specularSum / weightSum : specularTex.sample(v_texcoord0).xyz();
+				vec3 f0 = mix(vec3_splat(0.04f), albedo, metallic);
+				indirect += specularRadiance * specularAlbedo(f0, roughness, max(dot(normal, viewDirection), 0.001f))
+					* emissiveOcclusion.w * P->composite_specular;
+			}
 			vec3 result = direct * options[0] + indirect * options[1] + emissiveOcclusion.xyz() * options[3];
 			storeH4(hdr, i, vec4(result, 1.0f));
 		}
@@ -1614,6 +1651,213 @@ extern "C" void oracle_grid_keys(const float* camera, const float* constants, ui
 		g.key(jittered, nrm, size, slots[i], checksums[i]);
 		cell_bits[i] = floatBitsToUint(size);
 	}
+}
+
+/* --- indirect specular (fs_specular.sc) ---------------------------------- */
+
+namespace
+{
+
+void tangentFrame(vec3 _normal, vec3& _tangent, vec3& _bitangent)
+{
+	_tangent = normalize(abs(_normal.y) < 0.99f
+		? cross(_normal, vec3(0.0f, 1.0f, 0.0f))
+		: cross(_normal, vec3(1.0f, 0.0f, 0.0f)));
+	_bitangent = cross(_normal, _tangent);
+}
+
+vec3 sampleVisibleNormal(vec3 _view, float _alpha, float _random0, float _random1)
+{
+	vec3 stretched = normalize(vec3(_alpha * _view.x, _alpha * _view.y, _view.z));
+	float lengthSquared = stretched.x * stretched.x + stretched.y * stretched.y;
+	vec3 t1 = lengthSquared > 0.0f
+		? vec3(-stretched.y, stretched.x, 0.0f) * inversesqrt(lengthSquared)
+		: vec3(1.0f, 0.0f, 0.0f);
+	vec3 t2 = cross(stretched, t1);
+	float radius = sqrt(_random0);
+	float angle = 2.0f * kPi * _random1;
+	float p1 = radius * cos(angle);
+	float p2 = radius * sin(angle);
+	float s = 0.5f * (1.0f + stretched.z);
+	p2 = (1.0f - s) * sqrt(max(1.0f - p1 * p1, 0.0f)) + s * p2;
+	vec3 normal = p1 * t1 + p2 * t2 + sqrt(max(1.0f - p1 * p1 - p2 * p2, 0.0f)) * stretched;
+	return normalize(vec3(_alpha * normal.x, _alpha * normal.y, max(normal.z, 0.0f)));
+}
+
+float smithG1(float _cosine, float _alpha)
+{
+	float alphaSquared = _alpha * _alpha;
+	return 2.0f * _cosine / (_cosine + sqrt(alphaSquared + (1.0f - alphaSquared) * _cosine * _cosine));
+}
+
+vec3 reflect(vec3 _incident, vec3 _normal)
+{
+	return _incident - 2.0f * dot(_normal, _incident) * _normal;
+}
+
+/* fs_specular.sc:77-125 */
+vec3 hitRadiance(const GiPass& g, const TexH4& previousHdr, vec3 _hitPosition, float _hitId, vec3 _rayDirection)
+{
+	if (isSkySample(_hitId))
+	{
+		return g.sky.radiance(_rayDirection);
+	}
+	vec2 uv;
+	float viewDepth;
+	bool visibleSurface = false;
+	if (g.projectToScreen(_hitPosition, uv, viewDepth))
+	{
+		float depth = g.depthTex.sample(uv);
+		visibleSurface = depth < kSkyDepth
+			&& distance(g.reconstructWorldPosition(uv, depth), _hitPosition) <= g.kSampleTolerance();
+	}
+	if (visibleSurface)
+	{
+		vec4 clip = mul(g.screen.prevViewProj, vec4(_hitPosition, 1.0f));
+		if (g.P->history_valid > 0.5f && clip.w > 0.0001f)
+		{
+			vec2 previousUv = g.screen.clipToUv(clip);
+			vec4 previous = previousHdr.sample(previousUv);
+			if (isOnScreen(previousUv) && previous.w > 0.5f)
+			{
+				return previous.xyz();
+			}
+		}
+		vec3 normal = g.decodeNormal(uv);
+		return g.evaluateSecondaryDirect(uv, _hitPosition, normal)
+			+ g.previousIndirect(_hitPosition, normal, g.diffuseAlbedo(uv))
+			+ g.surfaceLight.sample(uv).xyz() * g.P->surface_light_scale;
+	}
+	int triangleIndex = int(abs(_hitId) + 0.5f) - 1;
+	if (triangleIndex < 0 || !g.bvh.available())
+	{
+		return vec3_splat(0.0f);
+	}
+	vec3 v0 = g.bvh.vertex(triangleIndex, 0);
+	vec3 normal = normalize(cross(g.bvh.vertex(triangleIndex, 1) - v0, g.bvh.vertex(triangleIndex, 2) - v0));
+	normal = dot(normal, -_rayDirection) < 0.0f ? -normal : normal;
+	vec3 albedo = bvhTriangleAlbedo(g.bvh, triangleIndex);
+	return g.evaluateWorldDirect(albedo, _hitPosition, normal)
+		+ g.previousIndirect(_hitPosition, normal, albedo)
+		+ bvhTriangleEmission(g.bvh, triangleIndex) * g.P->emission_scale;
+}
+
+} // namespace
+
+/* fs_specular.sc:127-226 at GI resolution. */
+extern "C" int oracle_gi_specular(const RestirParams* P, const RestirScene* scene, const RestirGBuffer* gb,
+	const RestirGiHistory* history, const float* shadow_atlas, const uint16_t* surface_light, const uint16_t* previous_hdr,
+	const uint16_t* specular_history, uint16_t* specular)
+{
+	resetCounts();
+	const GiPass base = makeGiPass(P, scene, gb, history, shadow_atlas, surface_light);
+	const int W = int(P->width), H = int(P->height);
+	const int w = int(P->gi_width), h = int(P->gi_height);
+	const TexH4 previousHdr = { previous_hdr, W, H };
+	const TexH4 specularHistory = { specular_history, w, h };
+	const vec3 camera(P->camera_position[0], P->camera_position[1], P->camera_position[2]);
+	parallelFor(int64_t(h), 4, [&](int64_t py_, int)
+	{
+		const GiPass& g = base;
+		const int py = int(py_);
+		for (int px = 0; px < w; ++px)
+		{
+			const int outIndex = py * w + px;
+			vec2 v_texcoord0 = (vec2(float(px), float(py)) + 0.5f) * g.giTexel;
+			float depth = g.depthTex.sample(v_texcoord0);
+			if (depth >= kSkyDepth)
+			{
+				storeH4(specular, outIndex, vec4_splat(0.0f));
+				continue;
+			}
+			vec3 position = g.reconstructWorldPosition(v_texcoord0, depth);
+			vec3 normal = g.decodeNormal(v_texcoord0);
+			vec4 albedoRoughness = g.albedoTex.sample(v_texcoord0);
+			float metallic = g.normalTex.sample(v_texcoord0).w;
+			float roughness = max(albedoRoughness.w, 0.02f);
+			float alpha = roughness * roughness;
+			vec3 viewDirection = normalize(camera - position);
+			float normalView = max(dot(normal, viewDirection), 0.001f);
+			vec3 f0 = mix(vec3_splat(0.04f), albedoRoughness.xyz(), metallic);
+			vec2 pixel = g.giPixel(v_texcoord0);
+			uint rng = pcg(uint(pixel.x) + pcg(uint(pixel.y) + pcg(uint(P->frame_index) ^ 0x2545f491u)));
+
+			vec3 tangent, bitangent;
+			tangentFrame(normal, tangent, bitangent);
+			vec3 localView = vec3(dot(viewDirection, tangent), dot(viewDirection, bitangent), normalView);
+			float random0 = nextRandom(rng);
+			float random1 = nextRandom(rng);
+			vec3 localHalfway = sampleVisibleNormal(localView, alpha, random0, random1);
+			vec3 halfway = tangent * localHalfway.x + bitangent * localHalfway.y + normal * localHalfway.z;
+			vec3 direction = reflect(-viewDirection, halfway);
+			float normalLight = dot(normal, direction);
+
+			vec3 estimate = vec3_splat(0.0f);
+			if (normalLight > 0.0f)
+			{
+				vec3 rayOrigin = position + normal * g.kRayBias();
+				vec3 hitPosition = vec3_splat(0.0f);
+				float hitId = 0.0f;
+				bool hit = false;
+				if (P->ray_mode != RESTIR_RAY_MODE_BVH)
+				{
+					hit = g.traceScreenSpaceRay(rayOrigin, direction, g.kMaxRayDistance(), hitPosition);
+				}
+				if (!hit && P->ray_mode != RESTIR_RAY_MODE_SCREEN)
+				{
+					float hitDistance = 0.0f;
+					int triangleIndex = traceBvh(g.bvh, rayOrigin, direction, g.kMaxBvhRayDistance(), false, hitDistance, false);
+					if (triangleIndex >= 0)
+					{
+						hit = true;
+						hitPosition = rayOrigin + direction * hitDistance;
+						hitId = g.encodeSampleId(triangleIndex, direction);
+					}
+					else if (g.sky.enabled())
+					{
+						hit = true;
+						hitId = kSkySampleId;
+					}
+				}
+				if (hit)
+				{
+					vec3 fresnel = fresnelSchlick(halfway, viewDirection, f0);
+					estimate = hitRadiance(g, previousHdr, hitPosition, hitId, direction) * fresnel * smithG1(normalLight, alpha);
+				}
+			}
+
+			vec3 demodulated = estimate / max(specularAlbedo(f0, roughness, normalView), vec3_splat(0.001f));
+			if (P->outlier_clamp > 0.0f)
+			{
+				demodulated = min(demodulated, vec3_splat(P->outlier_clamp));
+			}
+
+			vec3 pastColor = vec3_splat(0.0f);
+			float historyLength = 0.0f;
+			vec4 clipPrevious = mul(g.screen.prevViewProj, vec4(position, 1.0f));
+			if (P->history_valid > 0.5f && clipPrevious.w > 0.0001f)
+			{
+				vec2 previousUv = (floor(g.screen.clipToUv(clipPrevious) * g.giSize) + 0.5f) * g.giTexel;
+				vec3 receiverPosition = g.historyReceiver.sample(previousUv).xyz();
+				vec3 receiverNormal = g.historyNormal.sample(previousUv).xyz();
+				vec3 offset = receiverPosition - position;
+				if (isOnScreen(previousUv)
+					&& dot(receiverNormal, receiverNormal) > 0.5f
+					&& dot(offset, offset) <= g.kBounceRadius() * g.kBounceRadius()
+					&& abs(dot(offset, normal)) <= g.kReceiverPlane()
+					&& dot(normalize(receiverNormal), normal) >= 0.9f)
+				{
+					vec4 previous = specularHistory.sample(previousUv);
+					pastColor = previous.xyz();
+					historyLength = previous.w;
+				}
+			}
+			float maxHistory = mix(4.0f, 32.0f, clamp(roughness * 1.5f, 0.0f, 1.0f));
+			historyLength = min(historyLength + 1.0f, maxHistory);
+			storeH4(specular, outIndex, vec4(mix(pastColor, demodulated, 1.0f / historyLength), historyLength));
+		}
+	});
+	return RESTIR_OK;
 }
 
 extern "C" void oracle_numeric_eval(int fn, const float* input, float* output, uint32_t n)

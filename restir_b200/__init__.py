@@ -35,7 +35,7 @@ ERROR_TIMEOUT, ERROR_OUT_OF_MEMORY, ERROR_TOO_LARGE = -5, -6, -7
 TRACE_CLOSEST, TRACE_ANY, TRACE_CLOSEST_STACKLESS, TRACE_CLOSEST_WATERTIGHT, TRACE_CLOSEST_QUEUE = 0, 1, 2, 3, 4
 TRACE_ANY_WAVE = 5
 PASS_NAMES = ["shadow", "gbuffer", "di_temporal", "di_spatial", "grid", "gi_temporal", "gi_spatial",
-              "denoise", "composite", "reference", "cache", "display"]
+              "denoise", "composite", "reference", "cache", "display", "specular"]
 
 _lib = None
 
@@ -65,6 +65,9 @@ _SIGNATURES = {
     "restir_svgf_variance": (C.c_int, [C.POINTER(RestirParams), P, P, P, P, P, P]),
     "restir_svgf_atrous": (C.c_int, [C.POINTER(RestirParams), C.c_int, P, P, P, P, P]),
     "restir_composite": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirGBuffer), P, P, P, P, P, P]),
+    "restir_composite_specular": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirGBuffer), P, P, P, P, P, P, P]),
+    "restir_gi_specular": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirScene), C.POINTER(RestirGBuffer),
+                                     C.POINTER(RestirGiHistory), P, P, P, P, P, P]),
     "restir_reference_accumulate": (C.c_int, [C.POINTER(RestirParams), P, P, P, u32, P]),
     "restir_error_scratch_bytes": (C.c_uint64, [u32, u32]),
     "restir_error": (C.c_int, [C.POINTER(RestirParams), P, P, P, P, P, P]),

@@ -36,7 +36,7 @@ class RestirParams(C.Structure):
         ("sky_zenith", f4), ("sky_horizon", f4), ("sky_ground", f4),
         ("composite_options", f4),
         ("radiance_cache", C.c_float), ("cache_training_samples", C.c_uint32), ("wave_visibility", C.c_float),
-        ("pad_params", C.c_float * 1),
+        ("composite_specular", C.c_float),
     ]
 
 
@@ -106,7 +106,7 @@ class RestirSettings(C.Structure):
         ("wavefront", C.c_uint32), ("radiance_cache", C.c_uint32), ("cache_training_samples", C.c_uint32),
         ("wave_visibility", C.c_uint32),
         ("taa", C.c_int), ("auto_exposure", C.c_int), ("tonemapper", C.c_int), ("exposure_ev", C.c_float),
-        ("adaptation_speed", C.c_float), ("display", C.c_int), ("bvh_on_device", C.c_int),
+        ("adaptation_speed", C.c_float), ("display", C.c_int), ("bvh_on_device", C.c_int), ("specular_gi", C.c_int),
     ]
 
 
@@ -126,7 +126,7 @@ class RestirFrameState(C.Structure):
 
 class RestirMetrics(C.Structure):
     _fields_ = [("valid", C.c_int), ("relative_mse", C.c_double), ("bias", C.c_double), ("error", C.c_double * 4),
-                ("pass_ms", C.c_float * 12), ("reference_frames", C.c_uint32)]
+                ("pass_ms", C.c_float * 13), ("reference_frames", C.c_uint32)]
 
 
 class RestirFramePlan(C.Structure):
@@ -135,6 +135,7 @@ class RestirFramePlan(C.Structure):
         ("di_active", C.c_int), ("denoiser", C.c_int), ("atrous_iterations", C.c_int),
         ("reference_accumulate", C.c_int), ("reference_weight_frames", C.c_uint32),
         ("surface_light_is_di", C.c_int), ("display", C.c_int), ("taa", C.c_int), ("exposure", C.c_int),
+        ("specular", C.c_int),
         ("unjittered_view_proj", m16),
     ]
 

@@ -622,6 +622,218 @@ __global__ void __launch_bounds__(kGiThreads, RESTIR_GI_TEMPORAL_MIN_BLOCKS) giT
 	temporalReuseAndStore(P, g, b, lane, inside, working, px, py, position, normal, albedo, canonical, rng);
 }
 
+// --- indirect specular (fs_specular.sc) --------------------------------------------------
+
+// fs_specular.sc:41-47
+__device__ __forceinline__ void tangentFrame(V3 n, V3& tangent, V3& bitangent)
+{
+	tangent = normalize(fabsf(n.y) < 0.99f ? cross(n, v3(0.0f, 1.0f, 0.0f)) : cross(n, v3(1.0f, 0.0f, 0.0f)));
+	bitangent = cross(n, tangent);
+}
+
+// GGX visible normals (Heitz 2018), fs_specular.sc:51-67.
+__device__ __forceinline__ V3 sampleVisibleNormal(V3 view, float alpha, float random0, float random1)
+{
+	const V3 stretched = normalize(v3(alpha * view.x, alpha * view.y, view.z));
+	const float lengthSquared = stretched.x * stretched.x + stretched.y * stretched.y;
+	const V3 t1 = lengthSquared > 0.0f ? v3(-stretched.y, stretched.x, 0.0f) * inversesqrt(lengthSquared) : v3(1.0f, 0.0f, 0.0f);
+	const V3 t2 = cross(stretched, t1);
+	const float radius = sqrtf(random0);
+	const float angle = 2.0f * kPi * random1;
+	float sn, cs;
+	rn_sincos(angle, &sn, &cs);
+	const float p1 = radius * cs;
+	float p2 = radius * sn;
+	const float s = 0.5f * (1.0f + stretched.z);
+	p2 = (1.0f - s) * sqrtf(fmaxf(1.0f - p1 * p1, 0.0f)) + s * p2;
+	const V3 normal = t1 * p1 + t2 * p2 + stretched * sqrtf(fmaxf(1.0f - p1 * p1 - p2 * p2, 0.0f));
+	return normalize(v3(alpha * normal.x, alpha * normal.y, fmaxf(normal.z, 0.0f)));
+}
+
+// fs_specular.sc:70-74
+__device__ __forceinline__ float smithG1(float cosine, float alpha)
+{
+	const float alphaSquared = alpha * alpha;
+	return 2.0f * cosine / (cosine + sqrtf(alphaSquared + (1.0f - alphaSquared) * cosine * cosine));
+}
+
+// brdf.sh:29-37
+__device__ __forceinline__ V3 fresnelSchlick(V3 halfway, V3 view, V3 f0)
+{
+	const float cosine = clampf(dot(halfway, view), 0.0f, 1.0f);
+	return f0 + (v3s(1.0f) - f0) * rn_pow5(1.0f - cosine);
+}
+
+// The split-sum specular albedo, brdf.sh:68-76 (Karis' analytic fit).
+__device__ __forceinline__ V3 specularAlbedo(V3 f0, float roughness, float normalView)
+{
+	const float rx = -1.0f * roughness + 1.0f, ry = -0.0275f * roughness + 0.0425f;
+	const float rz = -0.572f * roughness + 1.04f, rw = 0.022f * roughness + -0.04f;
+	const float a004 = fminf(rx * rx, rn_exp2(-9.28f * normalView)) * rx + ry;
+	const float scale = -1.04f * a004 + rz, bias = 1.04f * a004 + rw;
+	return f0 * scale + bias;
+}
+
+// Radiance leaving a ray's hit point back along the ray, fs_specular.sc:77-125.
+__device__ inline V3 specularHitRadiance(const GiPass& g, const uint16_t* __restrict__ previousHdr, V3 hitPosition,
+	float hitId, V3 rayDirection)
+{
+	const RestirParams& P = g.P;
+	if (isSkySample(hitId))
+	{
+		return skyRadiance(P, rayDirection);
+	}
+	V2 uv;
+	float viewDepth;
+	bool visibleSurface = false;
+	if (g.projectToScreen(hitPosition, uv, viewDepth))
+	{
+		const float depth = g.depthAt(uv);
+		visibleSurface = depth < kSkyDepth && distance(reconstructWorldPosition(P, uv, depth), hitPosition) <= g.kSampleTolerance();
+	}
+	if (visibleSurface)
+	{
+		const V4 clip = mul(P.prev_view_proj, v4(hitPosition, 1.0f));
+		if (P.history_valid > 0.5f && clip.w > 0.0001f)
+		{
+			const V2 previousUv = clipToUv(P, clip);
+			const V4 previous = loadH4(previousHdr, g.full(previousUv));
+			if (isOnScreen(previousUv) && previous.w > 0.5f)
+			{
+				return previous.xyz();
+			}
+		}
+		const V3 normal = g.decode(uv);
+		return g.directFromLight(g.diffuseAlbedo(uv), hitPosition, normal) + g.previousIndirect(hitPosition, normal, g.diffuseAlbedo(uv))
+			+ loadH4(g.surfaceLight, g.full(uv)).xyz() * P.surface_light_scale;
+	}
+	const int triangleIndex = int(fabsf(hitId) + 0.5f) - 1;
+	if (triangleIndex < 0 || !g.bvh.available())
+	{
+		return v3s(0.0f);
+	}
+	const V3 v0 = g.bvh.vertex(triangleIndex, 0);
+	V3 normal = normalize(cross(g.bvh.vertex(triangleIndex, 1) - v0, g.bvh.vertex(triangleIndex, 2) - v0));
+	if (dot(normal, -rayDirection) < 0.0f)
+	{
+		normal = -normal;
+	}
+	const V3 albedo = g.bvh.albedo(triangleIndex);
+	return g.directFromLight(albedo, hitPosition, normal) + g.previousIndirect(hitPosition, normal, albedo)
+		+ g.bvh.emission(triangleIndex) * P.emission_scale;
+}
+
+// fs_specular.sc:127-226, one thread per GI pixel in 16x8 tiles.
+__global__ void __launch_bounds__(128) giSpecularKernel(const RestirParams P, BvhView bvh, GiBindings b,
+	const uint16_t* __restrict__ previousHdr, const uint16_t* __restrict__ specularHistory, uint16_t* out)
+{
+	GiPass g = makePass(P, bvh, b, P.camera_position, nullptr, 0);
+	const int px = int(blockIdx.x * 16 + threadIdx.x % 16);
+	const int py = int(blockIdx.y * 8 + threadIdx.x / 16);
+	if (px >= g.w || py >= g.h)
+	{
+		return;
+	}
+	const int i = py * g.w + px;
+	const V2 uv = pixelUv(px, py, g.giTexel);
+	const float depth = g.depthAt(uv);
+	if (depth >= kSkyDepth)
+	{
+		storeH4(out, i, v4(0.0f, 0.0f, 0.0f, 0.0f));
+		return;
+	}
+	const V3 position = reconstructWorldPosition(P, uv, depth);
+	const V3 normal = g.decode(uv);
+	const V4 albedoRoughness = loadU8(g.albedoTex, g.full(uv));
+	const float metallic = loadU8(g.normalTex, g.full(uv)).w;
+	const float roughness = fmaxf(albedoRoughness.w, 0.02f);
+	const float alpha = roughness * roughness;
+	const V3 camera = v3(P.camera_position[0], P.camera_position[1], P.camera_position[2]);
+	const V3 viewDirection = normalize(camera - position);
+	const float normalView = fmaxf(dot(normal, viewDirection), 0.001f);
+	const V3 f0 = mix(v3s(0.04f), albedoRoughness.xyz(), metallic);
+	const V2 pixel = v2(floorf(uv.x * g.giSize.x), floorf(uv.y * g.giSize.y));
+	uint32_t rng = pcg(uint32_t(pixel.x) + pcg(uint32_t(pixel.y) + pcg(uint32_t(P.frame_index) ^ 0x2545f491u)));
+
+	V3 tangent, bitangent;
+	tangentFrame(normal, tangent, bitangent);
+	const V3 localView = v3(dot(viewDirection, tangent), dot(viewDirection, bitangent), normalView);
+	const float random0 = nextRandom(rng);
+	const float random1 = nextRandom(rng);
+	const V3 localHalfway = sampleVisibleNormal(localView, alpha, random0, random1);
+	const V3 halfway = tangent * localHalfway.x + bitangent * localHalfway.y + normal * localHalfway.z;
+	const V3 incident = -viewDirection;
+	const V3 direction = incident - halfway * (2.0f * dot(halfway, incident));
+	const float normalLight = dot(normal, direction);
+
+	V3 estimate = v3s(0.0f);
+	if (normalLight > 0.0f)
+	{
+		const V3 rayOrigin = position + normal * g.kRayBias();
+		V3 hitPosition = v3s(0.0f);
+		float hitId = 0.0f;
+		bool hit = false;
+		if (P.ray_mode != RESTIR_RAY_MODE_BVH)
+		{
+			hit = g.traceScreenSpaceRay(rayOrigin, direction, g.kMaxRayDistance(), hitPosition);
+		}
+		if (!hit && P.ray_mode != RESTIR_RAY_MODE_SCREEN)
+		{
+			float hitDistance = 0.0f;
+			// A fragment shader: no shared-memory stack, the stackless walk (bvh.sh:298-319).
+			const int triangleIndex = traceBvh(g.bvh, rayOrigin, direction, g.kMaxBvhRayDistance(), false, hitDistance, nullptr, 0);
+			if (triangleIndex >= 0)
+			{
+				hit = true;
+				hitPosition = rayOrigin + direction * hitDistance;
+				hitId = g.encodeSampleId(triangleIndex, direction);
+			}
+			else if (skyEnabled(P))
+			{
+				hit = true;
+				hitId = kSkySampleId;
+			}
+		}
+		if (hit)
+		{
+			const V3 fresnel = fresnelSchlick(halfway, viewDirection, f0);
+			estimate = specularHitRadiance(g, previousHdr, hitPosition, hitId, direction) * fresnel * smithG1(normalLight, alpha);
+		}
+	}
+	V3 demodulated = estimate / vmax(specularAlbedo(f0, roughness, normalView), v3s(0.001f));
+	if (P.outlier_clamp > 0.0f)
+	{
+		demodulated = vmin(demodulated, v3s(P.outlier_clamp));
+	}
+
+	V3 history = v3s(0.0f);
+	float historyLength = 0.0f;
+	const V4 clipPrevious = mul(P.prev_view_proj, v4(position, 1.0f));
+	if (P.history_valid > 0.5f && clipPrevious.w > 0.0001f)
+	{
+		const V2 projected = clipToUv(P, clipPrevious);
+		const V2 previousUv = v2((floorf(projected.x * g.giSize.x) + 0.5f) * g.giTexel.x,
+			(floorf(projected.y * g.giSize.y) + 0.5f) * g.giTexel.y);
+		const int h = g.gi(previousUv);
+		const float4 rp = __ldg(g.historyReceiver + h);
+		const float4 rn = __ldg(g.historyNormal + h);
+		const V3 receiverPosition = v3(rp.x, rp.y, rp.z);
+		const V3 receiverNormal = v3(rn.x, rn.y, rn.z);
+		const V3 offset = receiverPosition - position;
+		if (isOnScreen(previousUv) && dot(receiverNormal, receiverNormal) > 0.5f
+			&& dot(offset, offset) <= g.kBounceRadius() * g.kBounceRadius() && fabsf(dot(offset, normal)) <= g.kReceiverPlane()
+			&& dot(normalize(receiverNormal), normal) >= 0.9f)
+		{
+			const V4 previous = loadH4(specularHistory, h);
+			history = previous.xyz();
+			historyLength = previous.w;
+		}
+	}
+	const float maxHistory = mixf(4.0f, 32.0f, clampf(roughness * 1.5f, 0.0f, 1.0f));
+	historyLength = fminf(historyLength + 1.0f, maxHistory);
+	storeH4(out, i, v4(mix(history, demodulated, 1.0f / historyLength), historyLength));
+}
+
 GiBindings bindings(const RestirGBuffer* gb, const RestirGiHistory* history, const uint32_t* grid, const float* shadowAtlas,
 	const uint16_t* surfaceLight)
 {
@@ -690,6 +902,25 @@ extern "C" int restir_gi_spatial(const RestirParams* params, const RestirScene* 
 	b.outMoments = moments;
 	dim3 grid((params->gi_width + 15) / 16, (params->gi_height + 7) / 8);
 	giSpatialKernel<<<grid, 128, 0, asStream(stream)>>>(*params, makeBvhView(scene), b);
+	return launchStatus();
+}
+
+extern "C" int restir_gi_specular(const RestirParams* params, const RestirScene* scene, const RestirGBuffer* gbuffer,
+	const RestirGiHistory* history, const float* shadow_atlas, const uint16_t* surface_light, const uint16_t* previous_hdr,
+	const uint16_t* specular_history, uint16_t* specular, void* stream)
+{
+	if (params == nullptr || scene == nullptr || gbuffer == nullptr || history == nullptr || shadow_atlas == nullptr
+		|| gbuffer->albedo == nullptr || gbuffer->normal == nullptr || gbuffer->depth == nullptr || history->receiver == nullptr
+		|| history->normal == nullptr || history->color == nullptr || previous_hdr == nullptr || specular_history == nullptr
+		|| specular == nullptr || specular == specular_history || params->gi_width == 0 || params->gi_height == 0
+		|| params->trace_steps <= 0)
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	GiBindings b = bindings(gbuffer, history, nullptr, shadow_atlas, surface_light);
+	dim3 grid((params->gi_width + 15) / 16, (params->gi_height + 7) / 8);
+	giSpecularKernel<<<grid, 128, 0, asStream(stream)>>>(*params, makeBvhView(scene), b, previous_hdr, specular_history,
+		specular);
 	return launchStatus();
 }
 

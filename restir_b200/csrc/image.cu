@@ -162,9 +162,21 @@ __global__ void __launch_bounds__(128) atrousKernel(const RestirParams P, int st
 	storeH4(out, i, v4(colorSum / weightSum, varianceSum / (weightSum * weightSum)));
 }
 
-// fs_composite.sc:48-143 with the final view's options and no specular GI.
+// The split-sum specular albedo, brdf.sh:68-76 (Karis' analytic fit).
+__device__ __forceinline__ V3 compositeSpecularAlbedo(V3 f0, float roughness, float normalView)
+{
+	const float rx = -1.0f * roughness + 1.0f, ry = -0.0275f * roughness + 0.0425f;
+	const float rz = -0.572f * roughness + 1.04f, rw = 0.022f * roughness + -0.04f;
+	const float a004 = fminf(rx * rx, rn_exp2(-9.28f * normalView)) * rx + ry;
+	const float scale = -1.04f * a004 + rz, bias = 1.04f * a004 + rw;
+	return f0 * scale + bias;
+}
+
+// fs_composite.sc:48-143 with the final view's options; the indirect
+// specular when a specular target is given.
 __global__ void __launch_bounds__(128) compositeKernel(const RestirParams P, RestirGBuffer gb, const float* __restrict__ atlas,
-	const uint16_t* __restrict__ gi, const uint16_t* __restrict__ diDiffuse, const uint16_t* __restrict__ diSpecular, uint16_t* hdr)
+	const uint16_t* __restrict__ gi, const uint16_t* __restrict__ diDiffuse, const uint16_t* __restrict__ diSpecular,
+	const uint16_t* __restrict__ specularTarget, uint16_t* hdr)
 {
 	const int W = int(P.width), H = int(P.height);
 	const int w = int(P.gi_width), h = int(P.gi_height);
@@ -239,6 +251,7 @@ __global__ void __launch_bounds__(128) compositeKernel(const RestirParams P, Res
 	const V2 blend = texelCoord - baseCoord;
 	const V2 giTexel = v2(1.0f / float(w), 1.0f / float(h));
 	V3 sum = v3s(0.0f);
+	V3 specularSum = v3s(0.0f);
 	float weightSum = 0.0f;
 	for (int tapIndex = 0; tapIndex < 4; ++tapIndex)
 	{
@@ -256,11 +269,23 @@ __global__ void __launch_bounds__(128) compositeKernel(const RestirParams P, Res
 		const float weight = (bilinear.x * bilinear.y + 0.01f) * stepf(fabsf(dot(tapPosition - position, surfaceNormal)), 0.03f * s)
 			* stepf(0.9f, dot(tapNormal, surfaceNormal));
 		sum = sum + loadH4(gi, texelIndex(tapUv, w, h)).xyz() * weight;
+		if (specularTarget != nullptr)
+		{
+			specularSum = specularSum + loadH4(specularTarget, texelIndex(tapUv, w, h)).xyz() * weight;
+		}
 		weightSum += weight;
 	}
 	const V3 irradiance = weightSum > 0.0f ? sum / weightSum : loadH4(gi, texelIndex(uv, w, h)).xyz();
-	const V3 indirect = irradiance
+	V3 indirect = irradiance
 		* (P.composite_options[2] > 0.5f ? albedo * (1.0f - metallic) * emissiveOcclusion.w : v3s(1.0f));
+	if (specularTarget != nullptr)
+	{
+		// fs_composite.sc:131-136
+		const V3 specularRadiance = weightSum > 0.0f ? specularSum / weightSum
+			: loadH4(specularTarget, texelIndex(uv, w, h)).xyz();
+		indirect = indirect + specularRadiance * compositeSpecularAlbedo(f0, roughness, fmaxf(dot(normal, viewDirection), 0.001f))
+			* emissiveOcclusion.w * P.composite_specular;
+	}
 	const V3 result = direct * P.composite_options[0] + indirect * P.composite_options[1]
 		+ emissiveOcclusion.xyz() * P.composite_options[3];
 	storeH4(hdr, i, v4(result, 1.0f));
@@ -309,6 +334,23 @@ extern "C" int restir_composite(const RestirParams* params, const RestirGBuffer*
 		return RESTIR_ERROR_INVALID_ARGUMENT;
 	}
 	dim3 grid((params->width + 15) / 16, (params->height + 7) / 8);
-	compositeKernel<<<grid, 128, 0, asStream(stream)>>>(*params, *gbuffer, shadow_atlas, gi, di_diffuse, di_specular, hdr);
+	compositeKernel<<<grid, 128, 0, asStream(stream)>>>(*params, *gbuffer, shadow_atlas, gi, di_diffuse, di_specular, nullptr,
+		hdr);
+	return launchStatus();
+}
+
+extern "C" int restir_composite_specular(const RestirParams* params, const RestirGBuffer* gbuffer, const float* shadow_atlas,
+	const uint16_t* gi, const uint16_t* di_diffuse, const uint16_t* di_specular, const uint16_t* specular, uint16_t* hdr,
+	void* stream)
+{
+	if (params == nullptr || gbuffer == nullptr || gbuffer->albedo == nullptr || gbuffer->normal == nullptr
+		|| gbuffer->emissive == nullptr || gbuffer->shading_normal == nullptr || gbuffer->depth == nullptr
+		|| shadow_atlas == nullptr || gi == nullptr || hdr == nullptr || params->width == 0 || params->height == 0)
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	dim3 grid((params->width + 15) / 16, (params->height + 7) / 8);
+	compositeKernel<<<grid, 128, 0, asStream(stream)>>>(*params, *gbuffer, shadow_atlas, gi, di_diffuse, di_specular, specular,
+		hdr);
 	return launchStatus();
 }

@@ -94,6 +94,7 @@ extern "C" void restir_settings_default(RestirSettings* s)
 	s->adaptation_speed = 1.5f;
 	s->display = 1;
 	s->bvh_on_device = 1;
+	s->specular_gi = 1;
 }
 
 extern "C" int restir_frame_params(const RestirSettings* requested, const RestirMeshDesc* scene, uint32_t light_count,
@@ -211,6 +212,7 @@ extern "C" int restir_frame_params(const RestirSettings* requested, const Restir
 	p->cache_training_samples = s.cache_training_samples < RESTIR_CACHE_MAX_BATCH ? s.cache_training_samples
 		: RESTIR_CACHE_MAX_BATCH;
 	p->wave_visibility = s.wave_visibility ? 1.0f : 0.0f;
+	p->composite_specular = s.specular_gi ? 1.0f : 0.0f;
 
 	// The shadow atlas (renderer.cpp:527-593): six faces of a slightly wider
 	// field of view than 90 degrees, a border of 4 texels.
@@ -259,6 +261,7 @@ extern "C" int restir_frame_params(const RestirSettings* requested, const Restir
 		plan->display = s.display ? 1 : 0;
 		plan->taa = taa ? 1 : 0;
 		plan->exposure = s.display && s.auto_exposure ? 1 : 0;
+		plan->specular = s.specular_gi ? 1 : 0;
 		copy16(plan->unjittered_view_proj, unjittered);
 	}
 	return RESTIR_OK;

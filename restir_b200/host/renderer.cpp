@@ -236,6 +236,10 @@ public:
 		restir_frame_advance(&m_params, &m_plan, &input, &m_state);
 		m_historyRead = 1 - m_historyRead;
 		m_displayTaa = m_plan.display && m_plan.taa;
+		if (m_plan.specular)
+		{
+			m_specularRead = 1 - m_specularRead;
+		}
 		if (m_displayTaa)
 		{
 			m_taaRead = 1 - m_taaRead;
@@ -591,6 +595,7 @@ private:
 			{ "filtered0", gi * 8 }, { "filtered1", gi * 8 }, { "filter0", gi * 8 }, { "filter1", gi * 8 },
 			{ "hdr", full * 8 }, { "reference.mean", full * 24 }, { "reference.alpha", full },
 			{ "taa0", full * 8 }, { "taa1", full * 8 }, { "display", full * 4 }, { "exposure", 64 },
+			{ "specular0", gi * 8 }, { "specular1", gi * 8 },
 			{ "error.scratch", errorScratchBytes() }, { "error.out", 64 },
 		};
 		for (const Spec& s : specs)
@@ -608,6 +613,7 @@ private:
 		m_historyRead = 0;
 		m_diRead = 0;
 		m_taaRead = 0;
+		m_specularRead = 0;
 		m_displayTaa = false;
 		m_state.history_valid = 0;
 		m_state.di_valid = 0;
@@ -788,6 +794,16 @@ private:
 			return restir_gi_spatial(&P, &scene, &gb, &current, gridWrite, &history, atlas, surface,
 				p<uint16_t>("gi.color" + H), p<uint16_t>("gi.moments" + H), s);
 		});
+		const std::string specularRead = "specular" + std::to_string(m_specularRead);
+		const std::string specularWrite = "specular" + std::to_string(1 - m_specularRead);
+		if (plan.specular)
+		{
+			// Indirect specular (renderer.cpp:835-855): last frame's composite and specular history.
+			run(RESTIR_PASS_SPECULAR, [&] {
+				return restir_gi_specular(&P, &scene, &gb, &history, atlas, surface, p<uint16_t>("hdr"),
+					p<uint16_t>(specularRead), p<uint16_t>(specularWrite), s);
+			});
+		}
 		if (cached)
 		{
 			// Training after the frame's queries: every query of a frame sees the same weights.
@@ -817,8 +833,8 @@ private:
 		const uint16_t* diDiffuse = plan.di_active ? p<uint16_t>("di.diffuse") : p<uint16_t>("black");
 		const uint16_t* diSpecular = plan.di_active ? p<uint16_t>("di.specular") : p<uint16_t>("black");
 		run(RESTIR_PASS_COMPOSITE, [&] {
-			return restir_composite(&P, &gb, atlas, p<uint16_t>(denoised), diDiffuse, diSpecular,
-				p<uint16_t>("hdr"), s);
+			return restir_composite_specular(&P, &gb, atlas, p<uint16_t>(denoised), diDiffuse, diSpecular,
+				plan.specular ? p<uint16_t>(specularWrite) : nullptr, p<uint16_t>("hdr"), s);
 		});
 		if (plan.reference_accumulate)
 		{
@@ -921,6 +937,7 @@ private:
 	int m_diRead = 0;
 	float m_deltaTime = 0.0f; // the frame input's delta_time (auto exposure)
 	int m_taaRead = 0;        // the TAA target holding last frame's output
+	int m_specularRead = 0;   // the specular target holding last frame's output
 	bool m_displayTaa = false; // the last frame's displayed HDR is its TAA output
 	bool m_timed = false;
 	// Per-pass events of the last kEventRing stream-launched frames.

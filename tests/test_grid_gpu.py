@@ -27,7 +27,7 @@ def run_grid(setup, params, gbuffer_host):
 @pytest.mark.gpu
 @pytest.mark.parametrize("scene,size,table", [((rb.SCENE_CORNELL, 0), (256, 256), 1 << 16),
                                               ((rb.SCENE_COURTYARD, 100000), (640, 360), 1 << 20),
-                                              ((rb.SCENE_CITY, 200000), (640, 360), 1 << 14)])
+                                              ((rb.SCENE_CITY, 200000), (640, 360), 1 << 15)])
 @pytest.mark.parametrize("mode", [rb.GRID_DETERMINISTIC, rb.GRID_ATOMIC])
 def test_grid_insert(scene, size, table, mode):
     setup = make_scene(*scene)
