@@ -411,6 +411,10 @@ def own_arm(args, rank: int, world: int) -> None:
 
     if args.quick:
         # Profiling runs: W warm-up frames, then K frames, nothing else.
+        if args.radiance_cache:
+            settings = renderer.settings
+            settings.radiance_cache = 1
+            renderer.settings = settings
         for _ in range(args.warmup):
             renderer.render(frame)
         for _ in range(args.steps):
@@ -557,6 +561,7 @@ def main():
                         help="the batched multi-view form (8 views of uneven resolution in one frame)")
     parser.add_argument("--cache-kernels", action="store_true",
                         help="time the radiance cache's query and training kernels alone (profiling)")
+    parser.add_argument("--radiance-cache", action="store_true", help="with --quick: the radiance-cache form")
     parser.add_argument("--bvh-build", action="store_true",
                         help="time the device BVH builder against the host builder (1M and 4M triangles)")
     parser.add_argument("--quick", action="store_true",
