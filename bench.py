@@ -276,6 +276,75 @@ def bvh_build(args) -> None:
     print(json.dumps({"bvh_build": lines, "steps": args.steps, "warmup": args.warmup}), flush=True)
 
 
+# The quality settings --pareto sweeps, each on top of the defaults.
+PARETO_VARIANTS = [
+    ("default", {}),
+    ("candidates1", {"initial_candidates": 1}),
+    ("spatial2", {"spatial_taps": 2}),
+    ("candidates1_spatial2", {"initial_candidates": 1, "spatial_taps": 2}),
+    ("no_specular", {"specular_gi": 0}),
+    ("atrous3", {"atrous_iterations": 3}),
+    ("cheapest", {"initial_candidates": 1, "spatial_taps": 2, "specular_gi": 0, "atrous_iterations": 3}),
+]
+# (GI resolution is not swept: the FP64 reference is rendered at the view's GI
+# resolution, so another divisor would be judged against another reference.)
+
+
+def pareto(args) -> None:
+    """--pareto: the metric's comparison at equal error. Both forms (plain and
+    radiance cache) over PARETO_VARIANTS on the 1920x1080 city view: device
+    ms/frame over `steps` frames (CUDA events) and the mean relMSE against the
+    same 64-frame FP64 reference over ERROR_FRAMES frames; then, per form, the
+    cheapest setting whose relMSE is within the plain default's."""
+    import torch
+    import restir_b200 as rb
+    mesh, settings = scene_and_settings(rb)
+    renderer = rb.Renderer(settings)
+    renderer.set_scene(mesh)
+    frame = rb.frame_input(mesh, WIDTH, HEIGHT)
+    renderer.set_reference_accumulation(True)
+    for _ in range(REFERENCE_FRAMES):
+        renderer.render(frame)
+    renderer.set_reference_accumulation(False)
+    base = dict(settings_fields(renderer.settings))
+    stream = torch.cuda.ExternalStream(renderer.stream)
+    rows = []
+    for form in ("plain", "cache"):
+        for name, changes in PARETO_VARIANTS:
+            s = renderer.settings
+            for field, value in {**base, **changes}.items():
+                setattr(s, field, value)
+            s.radiance_cache = 1 if form == "cache" else 0
+            renderer.settings = s
+            for _ in range(CACHE_TRAIN_FRAMES if form == "cache" else max(args.warmup, 20)):
+                renderer.render(frame)
+            start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            start.record(stream)
+            for _ in range(args.steps):
+                renderer.render(frame)
+            stop.record(stream)
+            torch.cuda.synchronize()
+            ms = start.elapsed_time(stop) / args.steps
+            error = error_stats(renderer, frame, ERROR_FRAMES)
+            rows.append({"form": form, "variant": name, "ms_per_frame": ms, "rel_mse": error["mean"]})
+    target = next(r["rel_mse"] for r in rows if r["form"] == "plain" and r["variant"] == "default")
+    best = {}
+    for form in ("plain", "cache"):
+        ok = [r for r in rows if r["form"] == form and r["rel_mse"] <= target]
+        best[form] = min(ok, key=lambda r: r["ms_per_frame"]) if ok else None
+    ratio = (best["plain"]["ms_per_frame"] / best["cache"]["ms_per_frame"]) if best["plain"] and best["cache"] else None
+    print(json.dumps({"pareto": rows, "target_rel_mse": target, "best": best,
+                      "plain_over_cache_at_equal_rel_mse": ratio, "steps": args.steps}), flush=True)
+    renderer.close()
+
+
+def settings_fields(settings):
+    """The (name, value) pairs of a RestirSettings (the variants start from these)."""
+    return [(name, getattr(settings, name)) for name, _ in type(settings)._fields_
+            if not hasattr(getattr(settings, name), "__len__")]
+
+
 BATCH_SIZES = [(640, 360), (960, 540), (1280, 720), (1920, 1080), (800, 450), (1600, 900), (1024, 576), (1440, 810)]
 
 
@@ -562,6 +631,8 @@ def main():
     parser.add_argument("--cache-kernels", action="store_true",
                         help="time the radiance cache's query and training kernels alone (profiling)")
     parser.add_argument("--radiance-cache", action="store_true", help="with --quick: the radiance-cache form")
+    parser.add_argument("--pareto", action="store_true",
+                        help="both forms over several quality settings: ms/frame and relMSE, best at equal error")
     parser.add_argument("--bvh-build", action="store_true",
                         help="time the device BVH builder against the host builder (1M and 4M triangles)")
     parser.add_argument("--quick", action="store_true",
@@ -574,6 +645,8 @@ def main():
         cache_kernels(args)
     elif args.bvh_build:
         bvh_build(args)
+    elif args.pareto:
+        pareto(args)
     elif args.batched:
         batched(args)
     elif args.impl == "reference":

@@ -1434,7 +1434,13 @@ __global__ void __launch_bounds__(128) trainingHitsKernel(const RestirParams P, 
 	c.hitAlbedo[j] = make_float4(albedo.x, albedo.y, albedo.z, 0.0f);
 }
 
-__global__ void __launch_bounds__(128) trainingTargetsKernel(CacheWorkspace c)
+// The training target: the light arriving along the suffix, i.e. its hit's
+// direct light and emission plus its albedo times the cache's value there.
+// With the outlier clamp on, the target is held to what the spatial pass
+// lets through at the training point (albedo x irradiance <= clamp,
+// cs_restir_spatial.sc:188-192): the same bias as the plain method, and a
+// bound on the loop through which the cache trains on its own values.
+__global__ void __launch_bounds__(128) trainingTargetsKernel(CacheWorkspace c, float outlierClamp)
 {
 	const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
 	if (j >= c.samples)
@@ -1445,8 +1451,15 @@ __global__ void __launch_bounds__(128) trainingTargetsKernel(CacheWorkspace c)
 	const float4 albedo = c.hitAlbedo[j];
 	const V4 cached = loadH4(c.hitValues, int(j));
 	const float beyond = cached.w > 0.5f ? 1.0f : 0.0f;
-	c.targets[j] = make_float4(partial.x + albedo.x * cached.x * beyond, partial.y + albedo.y * cached.y * beyond,
-		partial.z + albedo.z * cached.z * beyond, partial.w);
+	V3 target = v3(partial.x + albedo.x * cached.x * beyond, partial.y + albedo.y * cached.y * beyond,
+		partial.z + albedo.z * cached.z * beyond);
+	if (outlierClamp > 0.0f)
+	{
+		const float4 receiver = c.trainQueries[size_t(j) * 4 + 3];
+		target = v3(fminf(target.x, outlierClamp / fmaxf(receiver.x, 1e-4f)), fminf(target.y, outlierClamp / fmaxf(receiver.y, 1e-4f)),
+			fminf(target.z, outlierClamp / fmaxf(receiver.z, 1e-4f)));
+	}
+	c.targets[j] = make_float4(target.x, target.y, target.z, partial.w);
 }
 
 bool validCache(const RestirCacheConfig* cfg, const void* state)
@@ -1590,7 +1603,7 @@ extern "C" int restir_cache_train_frame(const RestirParams* params, const Restir
 	{
 		return status;
 	}
-	trainingTargetsKernel<<<gridFor(c.samples), 128, 0, s>>>(c);
+	trainingTargetsKernel<<<gridFor(c.samples), 128, 0, s>>>(c, params->outlier_clamp);
 	status = launchStatus();
 	if (status != RESTIR_OK)
 	{
