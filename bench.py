@@ -285,6 +285,11 @@ PARETO_VARIANTS = [
     ("no_specular", {"specular_gi": 0}),
     ("atrous3", {"atrous_iterations": 3}),
     ("cheapest", {"initial_candidates": 1, "spatial_taps": 2, "specular_gi": 0, "atrous_iterations": 3}),
+    # the cache-only GI (no GI rays: the cache at each GI pixel's surface); radiance-cache form only
+    ("cache_only", {"cache_only_gi": 1}),
+    ("cache_only_no_specular", {"cache_only_gi": 1, "specular_gi": 0}),
+    # diagnostic: no indirect light at all (how much of the error the GI term carries)
+    ("no_gi", {"initial_candidates": 0, "temporal_taps": 0, "spatial_taps": 0, "specular_gi": 0}),
 ]
 # (GI resolution is not swept: the FP64 reference is rendered at the view's GI
 # resolution, so another divisor would be judged against another reference.)
@@ -292,32 +297,36 @@ PARETO_VARIANTS = [
 
 def pareto(args) -> None:
     """--pareto: the metric's comparison at equal error. Both forms (plain and
-    radiance cache) over PARETO_VARIANTS on the 1920x1080 city view: device
-    ms/frame over `steps` frames (CUDA events) and the mean relMSE against the
-    same 64-frame FP64 reference over ERROR_FRAMES frames; then, per form, the
-    cheapest setting whose relMSE is within the plain default's."""
+    radiance cache) over PARETO_VARIANTS on the 1920x1080 city view, each pair
+    from a fresh renderer (fresh history and, for the cache form, a fresh
+    cache): the 64-frame FP64 reference with the default settings, then the
+    variant's settings, warm-up (CACHE_TRAIN_FRAMES of training for the cache
+    form), device ms/frame over `steps` frames (CUDA events) and the mean
+    relMSE over ERROR_FRAMES frames; then, per form, the cheapest setting
+    whose relMSE is within the plain default's."""
     import torch
     import restir_b200 as rb
     mesh, settings = scene_and_settings(rb)
-    renderer = rb.Renderer(settings)
-    renderer.set_scene(mesh)
     frame = rb.frame_input(mesh, WIDTH, HEIGHT)
-    renderer.set_reference_accumulation(True)
-    for _ in range(REFERENCE_FRAMES):
-        renderer.render(frame)
-    renderer.set_reference_accumulation(False)
-    base = dict(settings_fields(renderer.settings))
-    stream = torch.cuda.ExternalStream(renderer.stream)
     rows = []
     for form in ("plain", "cache"):
         for name, changes in PARETO_VARIANTS:
+            if form == "plain" and changes.get("cache_only_gi"):
+                continue
+            renderer = rb.Renderer(settings)
+            renderer.set_scene(mesh)
+            renderer.set_reference_accumulation(True)
+            for _ in range(REFERENCE_FRAMES):
+                renderer.render(frame)
+            renderer.set_reference_accumulation(False)
             s = renderer.settings
-            for field, value in {**base, **changes}.items():
+            for field, value in changes.items():
                 setattr(s, field, value)
             s.radiance_cache = 1 if form == "cache" else 0
             renderer.settings = s
             for _ in range(CACHE_TRAIN_FRAMES if form == "cache" else max(args.warmup, 20)):
                 renderer.render(frame)
+            stream = torch.cuda.ExternalStream(renderer.stream)
             start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             torch.cuda.synchronize()
             start.record(stream)
@@ -328,6 +337,7 @@ def pareto(args) -> None:
             ms = start.elapsed_time(stop) / args.steps
             error = error_stats(renderer, frame, ERROR_FRAMES)
             rows.append({"form": form, "variant": name, "ms_per_frame": ms, "rel_mse": error["mean"]})
+            renderer.close()
     target = next(r["rel_mse"] for r in rows if r["form"] == "plain" and r["variant"] == "default")
     best = {}
     for form in ("plain", "cache"):
@@ -336,7 +346,6 @@ def pareto(args) -> None:
     ratio = (best["plain"]["ms_per_frame"] / best["cache"]["ms_per_frame"]) if best["plain"] and best["cache"] else None
     print(json.dumps({"pareto": rows, "target_rel_mse": target, "best": best,
                       "plain_over_cache_at_equal_rel_mse": ratio, "steps": args.steps}), flush=True)
-    renderer.close()
 
 
 def settings_fields(settings):

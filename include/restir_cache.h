@@ -183,6 +183,18 @@ int restir_gi_spatial_cached(const RestirParams* params, const RestirScene* scen
 	const RestirCacheConfig* cache_config, const void* cache_state, void* workspace, uint64_t workspace_bytes,
 	void* stream);
 
+/* The cache-only form of the GI (no reference counterpart): the cache
+ * queried at every GI pixel's own surface, exactly as the training points
+ * query it (position, normal, view direction, roughness, diffuse albedo), in
+ * place of the GI temporal and spatial passes; no GI ray is traced. Writes
+ * the GI targets the later passes read: color (demodulated irradiance,
+ * clamped as the spatial pass clamps), moments, and the receiver and normal
+ * rows (sample rows zeroed). workspace: restir_gi_temporal_workspace_bytes
+ * with params->radiance_cache set. */
+int restir_gi_from_cache(const RestirParams* params, const RestirScene* scene, const RestirGBuffer* gbuffer,
+	const RestirCacheConfig* cache_config, const void* cache_state, void* workspace, uint64_t workspace_bytes,
+	const RestirGiReservoirs* output, uint16_t* color, uint16_t* moments, void* stream);
+
 /* One training step on params->cache_training_samples path suffixes: each
  * starts at a seeded GI pixel's G-buffer surface, takes a cosine-distributed
  * direction and its first hit through the BVH; the target is the light

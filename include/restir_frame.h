@@ -79,6 +79,9 @@ typedef struct RestirSettings
 	int bvh_on_device;       /* no reference counterpart: 1 builds the scene's BVH on the GPU
 	                            (restir_bvh_build_gpu, the same buffer), 0 on the host */
 	int specular_gi;         /* indirect specular (glossy reflections, settings.h:195) */
+	int cache_only_gi;       /* no reference counterpart: with radiance_cache, the GI is the
+	                            cache at each GI pixel's surface (restir_gi_from_cache): no GI
+	                            rays, no reuse, no denoiser */
 } RestirSettings;
 
 /* FrameInput (renderer.h) with the fly camera's pose. */
@@ -118,6 +121,7 @@ typedef struct RestirFramePlan
 	int taa;                      /* TAA runs: settings.taa, not while the reference accumulates */
 	int exposure;                 /* auto exposure runs */
 	int specular;                 /* restir_gi_specular runs and the composite adds it */
+	int gi_from_cache;            /* the cache-only GI replaces the GI temporal and spatial passes */
 	float unjittered_view_proj[16]; /* this frame's, for the next frame's TAA */
 } RestirFramePlan;
 

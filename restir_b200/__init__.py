@@ -66,6 +66,8 @@ _SIGNATURES = {
     "restir_svgf_atrous": (C.c_int, [C.POINTER(RestirParams), C.c_int, P, P, P, P, P]),
     "restir_composite": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirGBuffer), P, P, P, P, P, P]),
     "restir_composite_specular": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirGBuffer), P, P, P, P, P, P, P]),
+    "restir_gi_from_cache": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirScene), C.POINTER(RestirGBuffer), P, P, P,
+                                       C.c_uint64, C.POINTER(RestirGiReservoirs), P, P, P]),
     "restir_gi_specular": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirScene), C.POINTER(RestirGBuffer),
                                      C.POINTER(RestirGiHistory), P, P, P, P, P, P]),
     "restir_reference_accumulate": (C.c_int, [C.POINTER(RestirParams), P, P, P, u32, P]),

@@ -107,6 +107,7 @@ class RestirSettings(C.Structure):
         ("wave_visibility", C.c_uint32),
         ("taa", C.c_int), ("auto_exposure", C.c_int), ("tonemapper", C.c_int), ("exposure_ev", C.c_float),
         ("adaptation_speed", C.c_float), ("display", C.c_int), ("bvh_on_device", C.c_int), ("specular_gi", C.c_int),
+        ("cache_only_gi", C.c_int),
     ]
 
 
@@ -135,7 +136,7 @@ class RestirFramePlan(C.Structure):
         ("di_active", C.c_int), ("denoiser", C.c_int), ("atrous_iterations", C.c_int),
         ("reference_accumulate", C.c_int), ("reference_weight_frames", C.c_uint32),
         ("surface_light_is_di", C.c_int), ("display", C.c_int), ("taa", C.c_int), ("exposure", C.c_int),
-        ("specular", C.c_int),
+        ("specular", C.c_int), ("gi_from_cache", C.c_int),
         ("unjittered_view_proj", m16),
     ]
 

@@ -1362,6 +1362,70 @@ __global__ void __launch_bounds__(128) reservoirQueryKernel(const RestirParams P
 	sampleQuery(g, v3(r.x, r.y, r.z), v3(s.x, s.y, s.z), n.w, s.w > 0.0f, queries + size_t(i) * 4);
 }
 
+// The cache-only form: one row per GI pixel at its own G-buffer surface, the
+// query the training points use (trainingRaysKernel): the view direction,
+// the surface's roughness and diffuse albedo.
+__global__ void __launch_bounds__(128) primaryQueryKernel(const RestirParams P, BvhView bvh, GiBindings b, float4* queries)
+{
+	const int i = int(blockIdx.x * blockDim.x + threadIdx.x);
+	if (i >= int(P.gi_width * P.gi_height))
+	{
+		return;
+	}
+	GiPass g = makePass(P, bvh, b, P.camera_position, nullptr, 0);
+	const V2 uv = pixelUv(i % g.w, i / g.w, g.giTexel);
+	const float depth = g.depthAt(uv);
+	const V3 position = reconstructWorldPosition(P, uv, depth);
+	const V3 normal = g.decode(uv);
+	const V3 camera = v3(P.camera_position[0], P.camera_position[1], P.camera_position[2]);
+	const V3 toCamera = camera - position;
+	const float distanceSquared = dot(toCamera, toCamera);
+	const V3 view = distanceSquared > 0.0f ? toCamera * inversesqrt(distanceSquared) : normal;
+	writeQuery(queries + size_t(i) * 4, position, loadU8(g.albedoTex, g.full(uv)).w, normal, depth < kSkyDepth, view,
+		g.diffuseAlbedo(uv));
+}
+
+// The GI targets from the cache's values: demodulated irradiance (clamped as
+// the spatial pass clamps, albedo x irradiance <= the outlier clamp), its
+// moments for the denoiser, and the receiver rows the later passes read.
+__global__ void __launch_bounds__(128) giFromCacheKernel(const RestirParams P, BvhView bvh, GiBindings b,
+	const uint16_t* __restrict__ values, float4* outSample, float4* outReceiver, float4* outNormal, uint16_t* color,
+	uint16_t* moments)
+{
+	const int i = int(blockIdx.x * blockDim.x + threadIdx.x);
+	if (i >= int(P.gi_width * P.gi_height))
+	{
+		return;
+	}
+	GiPass g = makePass(P, bvh, b, P.camera_position, nullptr, 0);
+	const V2 uv = pixelUv(i % g.w, i / g.w, g.giTexel);
+	const float depth = g.depthAt(uv);
+	outSample[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+	if (depth >= kSkyDepth)
+	{
+		outReceiver[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+		outNormal[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+		storeH4(color, i, v4(0.0f, 0.0f, 0.0f, 0.0f));
+		storeH4(moments, i, v4(0.0f, 0.0f, 0.0f, 0.0f));
+		return;
+	}
+	const V3 position = reconstructWorldPosition(P, uv, depth);
+	const V3 normal = g.decode(uv);
+	const V4 value = loadH4(values, i);
+	V3 irradiance = value.w > 0.5f ? vmax(value.xyz(), v3s(0.0f)) : v3s(0.0f);
+	if (P.outlier_clamp > 0.0f)
+	{
+		const V3 albedo = g.diffuseAlbedo(uv);
+		irradiance = v3(fminf(irradiance.x, P.outlier_clamp / fmaxf(albedo.x, 1e-4f)),
+			fminf(irradiance.y, P.outlier_clamp / fmaxf(albedo.y, 1e-4f)), fminf(irradiance.z, P.outlier_clamp / fmaxf(albedo.z, 1e-4f)));
+	}
+	const float l = luminance(irradiance);
+	outReceiver[i] = make_float4(position.x, position.y, position.z, 1.0f);
+	outNormal[i] = make_float4(normal.x, normal.y, normal.z, 0.0f);
+	storeH4(color, i, v4(irradiance, 1.0f));
+	storeH4(moments, i, v4(l, l * l, 1.0f, 0.0f));
+}
+
 // Training: sample j starts at a seeded GI pixel's G-buffer surface and
 // traces one cosine-distributed suffix ray.
 __global__ void __launch_bounds__(128) trainingRaysKernel(const RestirParams P, BvhView bvh, GiBindings b, CacheWorkspace c)
@@ -1562,6 +1626,43 @@ extern "C" int restir_gi_spatial_cached(const RestirParams* params, const Restir
 	b.cacheNeighbourBase = 0;
 	dim3 grid((params->gi_width + 15) / 16, (params->gi_height + 7) / 8);
 	giSpatialKernel<<<grid, 128, 0, s>>>(*params, bvh, b);
+	return launchStatus();
+}
+
+extern "C" int restir_gi_from_cache(const RestirParams* params, const RestirScene* scene, const RestirGBuffer* gbuffer,
+	const RestirCacheConfig* cache_config, const void* cache_state, void* workspace, uint64_t workspace_bytes,
+	const RestirGiReservoirs* output, uint16_t* color, uint16_t* moments, void* stream)
+{
+	if (params == nullptr || scene == nullptr || gbuffer == nullptr || gbuffer->albedo == nullptr || gbuffer->normal == nullptr
+		|| gbuffer->depth == nullptr || output == nullptr || output->sample == nullptr || output->receiver == nullptr
+		|| output->normal == nullptr || color == nullptr || moments == nullptr || workspace == nullptr
+		|| (reinterpret_cast<uintptr_t>(workspace) & 255u) != 0u || params->radiance_cache <= 0.5f
+		|| params->gi_width == 0u || params->gi_height == 0u || !validCache(cache_config, cache_state))
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	TemporalWorkspace w = layoutTemporalWorkspace(params, workspace);
+	if (workspace_bytes < w.bytes)
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	GiBindings b = {};
+	b.albedo = gbuffer->albedo;
+	b.normal = gbuffer->normal;
+	b.depth = gbuffer->depth;
+	const BvhView bvh = makeBvhView(scene);
+	cudaStream_t s = asStream(stream);
+	const uint32_t pixels = params->gi_width * params->gi_height;
+	primaryQueryKernel<<<gridFor(pixels), 128, 0, s>>>(*params, bvh, b, w.cache.queries);
+	int status = restir_cache_query(cache_config, cache_state, reinterpret_cast<const float*>(w.cache.queries), pixels,
+		w.cache.values, stream);
+	if (status != RESTIR_OK)
+	{
+		return status;
+	}
+	giFromCacheKernel<<<gridFor(pixels), 128, 0, s>>>(*params, bvh, b, w.cache.values,
+		reinterpret_cast<float4*>(output->sample), reinterpret_cast<float4*>(output->receiver),
+		reinterpret_cast<float4*>(output->normal), color, moments);
 	return launchStatus();
 }
 

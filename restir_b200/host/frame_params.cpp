@@ -262,6 +262,11 @@ extern "C" int restir_frame_params(const RestirSettings* requested, const Restir
 		plan->taa = taa ? 1 : 0;
 		plan->exposure = s.display && s.auto_exposure ? 1 : 0;
 		plan->specular = s.specular_gi ? 1 : 0;
+		plan->gi_from_cache = p->radiance_cache > 0.5f && s.cache_only_gi ? 1 : 0;
+		if (plan->gi_from_cache)
+		{
+			plan->denoiser = 0; // the cache's values carry no sampling noise
+		}
 		copy16(plan->unjittered_view_proj, unjittered);
 	}
 	return RESTIR_OK;

@@ -742,7 +742,7 @@ private:
 		const uint16_t* surface = plan.surface_light_is_di ? (plan.di_active ? p<uint16_t>("di.diffuse") : p<uint16_t>("black"))
 			: p<uint16_t>("gbuffer.emissive");
 		uint32_t* gridWrite = p<uint32_t>("grid" + H);
-		if (before)
+		if (before && !plan.gi_from_cache)
 		{
 			run(RESTIR_PASS_GRID, [&] {
 				return restir_grid_clear(&P, gridWrite, s) | restir_grid_insert(&P, &gb, gridWrite, s);
@@ -767,6 +767,12 @@ private:
 		}
 		else run(RESTIR_PASS_GI_TEMPORAL, [&] {
 			const Buffer& w = m_targets["gi.workspace"];
+			if (plan.gi_from_cache)
+			{
+				// The cache-only form: the GI targets from the cache at each GI pixel's surface.
+				return restir_gi_from_cache(&P, &scene, &gb, &m_scene->cacheConfig, cacheState, w.pointer, w.bytes, &current,
+					p<uint16_t>("gi.color" + H), p<uint16_t>("gi.moments" + H), s);
+			}
 			if (cached)
 			{
 				return restir_gi_temporal_cached(&P, &scene, &gb, &history, p<uint32_t>("grid" + R), atlas,
@@ -784,7 +790,7 @@ private:
 		{
 			return status == RESTIR_OK ? RESTIR_OK : RESTIR_ERROR_LAUNCH;
 		}
-		run(RESTIR_PASS_GI_SPATIAL, [&] {
+		if (!plan.gi_from_cache) run(RESTIR_PASS_GI_SPATIAL, [&] {
 			if (cached)
 			{
 				const Buffer& w = m_targets["gi.workspace"];
