@@ -489,9 +489,12 @@ def own_arm(args, rank: int, world: int) -> None:
 
     if args.quick:
         # Profiling runs: W warm-up frames, then K frames, nothing else.
-        if args.radiance_cache:
+        if args.radiance_cache or args.set:
             settings = renderer.settings
-            settings.radiance_cache = 1
+            settings.radiance_cache = 1 if args.radiance_cache else settings.radiance_cache
+            for item in args.set:
+                name, value = item.split("=")
+                setattr(settings, name, type(getattr(settings, name))(float(value)))
             renderer.settings = settings
         for _ in range(args.warmup):
             renderer.render(frame)
@@ -640,6 +643,8 @@ def main():
     parser.add_argument("--cache-kernels", action="store_true",
                         help="time the radiance cache's query and training kernels alone (profiling)")
     parser.add_argument("--radiance-cache", action="store_true", help="with --quick: the radiance-cache form")
+    parser.add_argument("--set", action="append", default=[], metavar="NAME=VALUE",
+                        help="with --quick: a RestirSettings field (repeatable), e.g. --set cache_only_gi=1")
     parser.add_argument("--pareto", action="store_true",
                         help="both forms over several quality settings: ms/frame and relMSE, best at equal error")
     parser.add_argument("--bvh-build", action="store_true",

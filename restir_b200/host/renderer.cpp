@@ -78,6 +78,9 @@ public:
 			m_state.previous_view_proj[i * 5] = 1.0f;
 		}
 		cudaStreamCreateWithFlags(&m_stream, cudaStreamNonBlocking);
+		cudaStreamCreateWithFlags(&m_side, cudaStreamNonBlocking);
+		cudaEventCreateWithFlags(&m_fork, cudaEventDisableTiming);
+		cudaEventCreateWithFlags(&m_join, cudaEventDisableTiming);
 		for (auto& frame : m_events)
 		{
 			for (auto& pass : frame)
@@ -104,6 +107,10 @@ public:
 			}
 		}
 		cudaFreeHost(m_errorHost);
+		cudaStreamSynchronize(m_side);
+		cudaEventDestroy(m_fork);
+		cudaEventDestroy(m_join);
+		cudaStreamDestroy(m_side);
 		cudaStreamDestroy(m_stream);
 	}
 
@@ -729,6 +736,53 @@ private:
 		{
 			run(RESTIR_PASS_GBUFFER, [&] { return restir_gbuffer_primary(&P, &scene, &gb, s); });
 		}
+		const bool cached = P.radiance_cache > 0.5f;
+		void* cacheState = m_scene->buffers["cache.state"].pointer;
+		// The cache's training only reads the G-buffer, the shadow atlas and the
+		// cache: it runs on a side stream, forked once the frame's queries are
+		// enqueued (so they all see the same weights) and joined before the
+		// frame ends, overlapping the passes in between. A profiling frame keeps
+		// it on the main stream (its counters wait pass by pass).
+		bool joinSide = false;
+		auto train = [&]()
+		{
+			const Buffer& w = m_targets["gi.workspace"];
+			if (m_profile != nullptr)
+			{
+				run(RESTIR_PASS_CACHE, [&] {
+					return restir_cache_train_frame(&P, &scene, &gb, atlas, &m_scene->cacheConfig, cacheState, w.pointer,
+						w.bytes, s);
+				});
+				return;
+			}
+			cudaEventRecord(m_fork, m_stream);
+			cudaStreamWaitEvent(m_side, m_fork, 0);
+			if (events)
+			{
+				cudaEventRecord(m_events[m_slot][RESTIR_PASS_CACHE][0], m_side);
+			}
+			status |= restir_cache_train_frame(&P, &scene, &gb, atlas, &m_scene->cacheConfig, cacheState, w.pointer, w.bytes,
+				m_side);
+			m_passRan[m_slot][RESTIR_PASS_CACHE] = true;
+			if (events)
+			{
+				cudaEventRecord(m_events[m_slot][RESTIR_PASS_CACHE][1], m_side);
+			}
+			cudaEventRecord(m_join, m_side);
+			joinSide = true;
+		};
+		if (plan.gi_from_cache && part == kWholeFrame)
+		{
+			// The cache-only form's GI needs only the G-buffer: its queries first,
+			// then the training overlaps the DI passes.
+			RestirGiReservoirs current = { p<float>("gi.sample" + H), p<float>("gi.receiver" + H), p<float>("gi.normal" + H) };
+			run(RESTIR_PASS_GI_TEMPORAL, [&] {
+				const Buffer& w = m_targets["gi.workspace"];
+				return restir_gi_from_cache(&P, &scene, &gb, &m_scene->cacheConfig, cacheState, w.pointer, w.bytes, &current,
+					p<uint16_t>("gi.color" + H), p<uint16_t>("gi.moments" + H), s);
+			});
+			train();
+		}
 		const std::string DW = std::to_string(dw), DR = std::to_string(dr);
 		RestirDiReservoirs diPrevious = { p<float>("di.sample" + DR), p<float>("di.receiver" + DR), p<uint16_t>("di.normal" + DR) };
 		RestirDiReservoirs diCurrent = { p<float>("di.sample" + DW), p<float>("di.receiver" + DW), p<uint16_t>("di.normal" + DW) };
@@ -751,8 +805,6 @@ private:
 		RestirGiHistory history = { p<float>("gi.sample" + R), p<float>("gi.receiver" + R), p<float>("gi.normal" + R),
 			plan.denoiser ? p<uint16_t>("filtered" + R) : p<uint16_t>("gi.color" + R), p<uint16_t>("gi.moments" + R) };
 		RestirGiReservoirs current = { p<float>("gi.sample" + H), p<float>("gi.receiver" + H), p<float>("gi.normal" + H) };
-		const bool cached = P.radiance_cache > 0.5f;
-		void* cacheState = m_scene->buffers["cache.state"].pointer;
 		if (part != kWholeFrame)
 		{
 			// The batch's shared ray queue: candidates before its one tracer launch, shading after.
@@ -765,14 +817,8 @@ private:
 						r.pointer, r.bytes, m_batchQueue, m_batchQueueCapacity, s);
 			});
 		}
-		else run(RESTIR_PASS_GI_TEMPORAL, [&] {
+		else if (!plan.gi_from_cache) run(RESTIR_PASS_GI_TEMPORAL, [&] {
 			const Buffer& w = m_targets["gi.workspace"];
-			if (plan.gi_from_cache)
-			{
-				// The cache-only form: the GI targets from the cache at each GI pixel's surface.
-				return restir_gi_from_cache(&P, &scene, &gb, &m_scene->cacheConfig, cacheState, w.pointer, w.bytes, &current,
-					p<uint16_t>("gi.color" + H), p<uint16_t>("gi.moments" + H), s);
-			}
 			if (cached)
 			{
 				return restir_gi_temporal_cached(&P, &scene, &gb, &history, p<uint32_t>("grid" + R), atlas,
@@ -810,14 +856,10 @@ private:
 					p<uint16_t>(specularRead), p<uint16_t>(specularWrite), s);
 			});
 		}
-		if (cached)
+		if (cached && !plan.gi_from_cache)
 		{
 			// Training after the frame's queries: every query of a frame sees the same weights.
-			run(RESTIR_PASS_CACHE, [&] {
-				const Buffer& w = m_targets["gi.workspace"];
-				return restir_cache_train_frame(&P, &scene, &gb, atlas, &m_scene->cacheConfig, cacheState, w.pointer,
-					w.bytes, s);
-			});
+			train();
 		}
 		std::string denoised = "gi.color" + H;
 		if (plan.denoiser)
@@ -861,6 +903,10 @@ private:
 				return restir_display(&D, p<uint16_t>("hdr"), p<float>("gbuffer.depth"), p<uint16_t>(taaRead),
 					p<uint16_t>(taaWrite), p<uint32_t>("exposure"), nullptr, nullptr, p<uint8_t>("display"), s);
 			});
+		}
+		if (joinSide)
+		{
+			cudaStreamWaitEvent(m_stream, m_join, 0);
 		}
 		return status == RESTIR_OK ? RESTIR_OK : RESTIR_ERROR_LAUNCH;
 	}
@@ -954,6 +1000,8 @@ private:
 	uint32_t m_lastSlot = 0;
 	uint32_t m_timedFrames = 0;
 	cudaStream_t m_stream = nullptr;
+	cudaStream_t m_side = nullptr;   // the cache's training, overlapping the rest of the frame
+	cudaEvent_t m_fork = nullptr, m_join = nullptr;
 	cudaGraphExec_t m_graphExec = nullptr;
 	double* m_errorHost = nullptr;
 	uint64_t* m_profile = nullptr;

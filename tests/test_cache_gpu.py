@@ -193,3 +193,40 @@ def test_training_fits_target():
     # generalise to about 0.04.
     assert rel < 0.1, rel
     assert rb.status_flags() & 8 == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cache_only", [0, 1])
+def test_renderer_cache_forms_train_on_a_side_stream(cache_only):
+    """The renderer's radiance-cache forms (GI passes with the cache, and the
+    cache-only GI): training runs on a side stream overlapping the frame and
+    joins before it ends; the frames stay finite, the cache trains (step count
+    advances) and its pass is timed."""
+    import torch
+    from tests.helpers import make_scene
+    setup = make_scene(rb.SCENE_COURTYARD, 0, 20000)
+    settings = setup.settings
+    settings.radiance_cache = 1
+    settings.cache_only_gi = cache_only
+    settings.cache_training_samples = 4096
+    renderer = rb.Renderer(settings)
+    renderer.set_scene(setup.mesh)
+    frame = rb.frame_input(setup.mesh, 160, 96)
+    for _ in range(6):
+        renderer.render(frame)
+    renderer.synchronize()
+    assert rb.status_flags() & 8 == 0
+    params, plan, _ = renderer.last_frame()
+    assert plan.gi_from_cache == cache_only and params.radiance_cache == 1.0
+    hdr = renderer.download("display.hdr", np.float16)[:160 * 96 * 4].astype(np.float32)
+    assert np.all(np.isfinite(hdr))
+    gi = renderer.download("gi.color0", np.float16).astype(np.float32)
+    assert np.count_nonzero(gi) > 0
+    times = renderer.pass_history(3)
+    cache_index = rb.PASS_NAMES.index("cache")
+    assert np.all(times[:, cache_index] > 0.0)
+    layout = rb.cache_layout(rb.cache_config())
+    pointer, nbytes = renderer.buffer("cache.state")
+    raw = rb.device_view(pointer, nbytes, torch.uint8)[layout.scalars:layout.scalars + 64].cpu().numpy()
+    scalars = rb.abi.RestirCacheScalars.from_buffer_copy(raw[:C.sizeof(rb.abi.RestirCacheScalars)].tobytes())
+    assert scalars.step == 6
