@@ -45,7 +45,7 @@ WIDTH, HEIGHT = 1920, 1080
 TRIANGLES = 1_000_000
 EXTRA_LIGHTS = 64
 REFERENCE_FRAMES = 64
-ERROR_FRAMES = 30          # frames the relMSE is averaged over
+ERROR_FRAMES = 240         # frames the relMSE is averaged over (it swings by +-0.07 between 30-frame windows)
 # DRAM bytes (read + write) per frame of a pass's kernels, from the committed ncu capture of this
 # workload (profiles/gi_temporal_wavefront_1080p_city1M.md): candidates 15.9 MB, queue tracer
 # 30.7 MB, shading 83.9 MB.
@@ -429,14 +429,18 @@ def error_stats(renderer, frame, frames: int) -> dict:
     return {"mean": float(np.mean(values)), "median": float(np.median(values))}
 
 
-def cache_arm(renderer, frame, steps: int) -> dict:
-    """The radiance-cache form on the same view: CACHE_TRAIN_FRAMES frames of
-    online training, then `steps` timed frames (CUDA events on the renderer's
-    stream) and the relMSE over ERROR_FRAMES frames."""
+def cache_arm(renderer, frame, steps: int, changes: dict | None = None) -> dict:
+    """The radiance-cache form on the same view (with `changes` to the settings
+    on top, restored after): CACHE_TRAIN_FRAMES frames of online training,
+    then `steps` timed frames (CUDA events on the renderer's stream) and the
+    relMSE over ERROR_FRAMES frames."""
     import torch
     import restir_b200 as rb
     settings = renderer.settings
+    saved = {name: getattr(settings, name) for name in (changes or {})}
     settings.radiance_cache = 1
+    for name, value in (changes or {}).items():
+        setattr(settings, name, value)
     renderer.settings = settings
     for _ in range(CACHE_TRAIN_FRAMES):
         renderer.render(frame)
@@ -456,8 +460,10 @@ def cache_arm(renderer, frame, steps: int) -> dict:
     error = error_stats(renderer, frame, ERROR_FRAMES)
     params, _, _ = renderer.last_frame()
     settings.radiance_cache = 0
+    for name, value in saved.items():
+        setattr(settings, name, value)
     renderer.settings = settings
-    return {"ms_per_frame": ms, "rel_mse_vs_fp64_reference": error["mean"], "rel_mse_median": error["median"],
+    return {"ms_per_frame": ms, "settings": dict(changes or {}), "rel_mse_vs_fp64_reference": error["mean"], "rel_mse_median": error["median"],
             "training_frames": CACHE_TRAIN_FRAMES + steps, "training_samples_per_frame": int(params.cache_training_samples),
             "pass_ms": {name: float(mean_pass[i]) for i, name in enumerate(rb.PASS_NAMES)}}
 
@@ -553,6 +559,10 @@ def own_arm(args, rank: int, world: int) -> None:
     # radiance-cache form after it has trained.
     plain_error = error_stats(renderer, frame, ERROR_FRAMES)
     cache_line = cache_arm(renderer, frame, args.steps) if not args.no_cache else None
+    # The cache-only GI form at its cheapest setting of the --pareto sweep (the
+    # cache continues from the form above).
+    cache_only_line = (cache_arm(renderer, frame, args.steps, {"cache_only_gi": 1, "specular_gi": 0})
+                       if not args.no_cache else None)
 
     elapsed_ms, e2e_ms = max_over_ranks([elapsed_ms, e2e_ms], dist, "cuda")
     if rank != 0:
@@ -604,6 +614,12 @@ def own_arm(args, rank: int, world: int) -> None:
         "bias_vs_fp64_reference": metrics.bias, "rel_mse_frames": ERROR_FRAMES,
         "reference_frames": REFERENCE_FRAMES,
         "radiance_cache": cache_line,
+        "radiance_cache_only_gi": cache_only_line,
+        # The metric's comparison: plain ms/frame over the cache-only form's, when the
+        # latter's relMSE is within the plain method's (else null).
+        "plain_over_cache_at_equal_rel_mse": (ms_per_frame / cache_only_line["ms_per_frame"]
+                                              if cache_only_line and cache_only_line["rel_mse_vs_fp64_reference"]
+                                              <= plain_error["mean"] else None),
         "pass_ms": {name: float(mean_pass[i]) for i, name in enumerate(passes)},
         "pass_share": share,
         "pass_algorithmic_gbs": {name: (float(pass_bytes[name] / (mean_pass[i] * 1e-3) / 1e9) if mean_pass[i] > 0 else 0.0)

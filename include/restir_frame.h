@@ -82,6 +82,8 @@ typedef struct RestirSettings
 	int cache_only_gi;       /* no reference counterpart: with radiance_cache, the GI is the
 	                            cache at each GI pixel's surface (restir_gi_from_cache): no GI
 	                            rays, no reuse, no denoiser */
+	float cache_learning_rate; /* no reference counterpart: the cache's Adam step size
+	                              (0: restir_cache_config_default's) */
 } RestirSettings;
 
 /* FrameInput (renderer.h) with the fly camera's pose. */

@@ -177,13 +177,24 @@ public:
 			b.pointer = nullptr;
 			return 1;
 		}
+		applyCacheSettings();
 		return restir_cache_init(&m_scene->cacheConfig, b.pointer, m_stream) == RESTIR_OK ? 0 : 1;
 	}
 
 	int setSettings(const RestirSettings& settings)
 	{
 		m_settings = settings;
+		applyCacheSettings();
 		return updateLights();
+	}
+
+	// The settings the cache's training reads on every step.
+	void applyCacheSettings()
+	{
+		RestirCacheConfig defaults;
+		restir_cache_config_default(&defaults);
+		m_scene->cacheConfig.learning_rate = m_settings.cache_learning_rate > 0.0f ? m_settings.cache_learning_rate
+			: defaults.learning_rate;
 	}
 
 	const RestirSettings& settings() const { return m_settings; }
