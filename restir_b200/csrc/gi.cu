@@ -22,9 +22,11 @@ constexpr int kGiThreads = 32 * kGiWarps;
 // Minimum resident blocks per SM (register budget) of the two GI kernels.
 // Measured on the 1080p frame (launch-bound sweep): the spatial pass gains
 // from 8 blocks (64 registers, a little spilling to L1); the temporal pass is
-// bound by divergence, not occupancy, and keeps its registers.
+// bound by divergence more than occupancy: its wavefront form takes 3.00 ms
+// at its natural 150 registers (3 blocks), 2.97 / 2.96 / 2.91 ms at 4 / 5 / 6
+// blocks (6: 80 registers, 270 bytes spilled to L1).
 #ifndef RESTIR_GI_TEMPORAL_MIN_BLOCKS
-#	define RESTIR_GI_TEMPORAL_MIN_BLOCKS 1
+#	define RESTIR_GI_TEMPORAL_MIN_BLOCKS 6
 #endif
 #ifndef RESTIR_GI_SPATIAL_MIN_BLOCKS
 #	define RESTIR_GI_SPATIAL_MIN_BLOCKS 8
