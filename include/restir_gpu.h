@@ -346,6 +346,23 @@ int restir_gi_specular(const RestirParams* params, const RestirScene* scene, con
 	const RestirGiHistory* history, const float* shadow_atlas, const uint16_t* surface_light, const uint16_t* previous_hdr,
 	const uint16_t* specular_history, uint16_t* specular, void* stream);
 
+/* No reference counterpart: the bytes of device workspace that
+ * restir_gi_specular_wavefront needs for these params (56 bytes per GI
+ * pixel, in five regions each rounded up to 256). */
+uint64_t restir_gi_specular_workspace_bytes(const RestirParams* params);
+
+/* restir_gi_specular as a wavefront, with identical outputs: a rays pass
+ * (reflection directions and depth-buffer marches) appends the rays the
+ * march does not answer to a queue in the workspace, a persistent tracer
+ * runs the stackless walk over the queue (a lane takes the next ray as soon
+ * as its own ends), and a shading pass completes fs_specular.sc from the
+ * recorded hits. workspace: 256-byte aligned device memory of at least
+ * restir_gi_specular_workspace_bytes; it must not be shared with a call
+ * whose kernels may overlap this one's. */
+int restir_gi_specular_wavefront(const RestirParams* params, const RestirScene* scene, const RestirGBuffer* gbuffer,
+	const RestirGiHistory* history, const float* shadow_atlas, const uint16_t* surface_light, const uint16_t* previous_hdr,
+	const uint16_t* specular_history, uint16_t* specular, void* workspace, uint64_t workspace_bytes, void* stream);
+
 /* The running mean of the composite in FP64 (fs_reference.sc):
  * mean = mean * (1 - w) + color * w with w = 1 / (frames + 1), NaN colours
  * keep the mean. mean: 3 planes of width * height doubles (r, g, b);

@@ -51,9 +51,11 @@ class FrameRunner:
                  gi_wavefront: bool = False):
         self.setup = setup
         self.backend = backend
-        # cuda backend: the GI temporal pass through restir_gi_temporal_wavefront
+        # cuda backend: the GI temporal and specular passes through their
+        # wavefront forms (restir_gi_temporal_wavefront, restir_gi_specular_wavefront)
         self.gi_wavefront = gi_wavefront and backend == "cuda"
         self.gi_workspace = None
+        self.specular_workspace = None
         self.settings = settings or setup.settings
         self.width, self.height = width, height
         self.state = rb.initial_state()
@@ -174,7 +176,10 @@ class FrameRunner:
                                                         self.b(f"grid{hw}"), history, self.b("atlas"), surface,
                                                         self.b(f"gi.color{hw}"), self.b(f"gi.moments{hw}"))))
         specular_write = f"specular{1 - self.specular_read}"
-        if plan.specular:
+        if plan.specular and self.gi_wavefront:
+            out.append(("gi_specular", lambda: self.gi_specular_wavefront(
+                P, gb, history, surface, self.b(f"specular{self.specular_read}"), self.b(specular_write))))
+        elif plan.specular:
             # Indirect specular (renderer.cpp:835-855): last frame's composite and specular history.
             out.append(("gi_specular", lambda: self.call(
                 "gi_specular", P, self.scene, gb, history, self.b("atlas"), surface, self.b("hdr"),
@@ -237,6 +242,17 @@ class FrameRunner:
         rb.check(self.lib.restir_gi_temporal_wavefront(P, self.scene, gb, history, grid, self.b("atlas"), surface,
                                                         current, self.gi_workspace.data_ptr(), nbytes, None),
                  "gi_temporal_wavefront")
+
+    def gi_specular_wavefront(self, P, gb, history, surface, specular_read, specular_write):
+        import torch
+        nbytes = int(self.lib.restir_gi_specular_workspace_bytes(P))
+        if self.specular_workspace is None or self.specular_workspace.numel() < nbytes:
+            self.specular_workspace = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+        assert self.specular_workspace.data_ptr() % 256 == 0
+        rb.check(self.lib.restir_gi_specular_wavefront(P, self.scene, gb, history, self.b("atlas"), surface,
+                                                        self.b("hdr"), specular_read, specular_write,
+                                                        self.specular_workspace.data_ptr(), nbytes, None),
+                 "gi_specular_wavefront")
 
     def workspace(self, P):
         import torch

@@ -70,6 +70,10 @@ _SIGNATURES = {
                                        C.c_uint64, C.POINTER(RestirGiReservoirs), P, P, P]),
     "restir_gi_specular": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirScene), C.POINTER(RestirGBuffer),
                                      C.POINTER(RestirGiHistory), P, P, P, P, P, P]),
+    "restir_gi_specular_workspace_bytes": (C.c_uint64, [C.POINTER(RestirParams)]),
+    "restir_gi_specular_wavefront": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirScene),
+                                               C.POINTER(RestirGBuffer), C.POINTER(RestirGiHistory), P, P, P, P, P,
+                                               P, C.c_uint64, P]),
     "restir_reference_accumulate": (C.c_int, [C.POINTER(RestirParams), P, P, P, u32, P]),
     "restir_error_scratch_bytes": (C.c_uint64, [u32, u32]),
     "restir_error": (C.c_int, [C.POINTER(RestirParams), P, P, P, P, P, P]),

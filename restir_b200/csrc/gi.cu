@@ -732,6 +732,115 @@ __device__ inline V3 specularHitRadiance(const GiPass& g, const uint16_t* __rest
 #define RESTIR_SPECULAR_MIN_BLOCKS 8
 #endif
 
+// The pixel's surface and its reflection ray, fs_specular.sc:127-160.
+struct SpecularRay
+{
+	bool surface;
+	V3 position, normal, viewDirection, f0, halfway, direction, origin;
+	float roughness, alpha, normalView, normalLight;
+};
+
+__device__ __forceinline__ SpecularRay specularRay(const GiPass& g, V2 uv)
+{
+	const RestirParams& P = g.P;
+	SpecularRay r;
+	const float depth = g.depthAt(uv);
+	r.surface = depth < kSkyDepth;
+	if (!r.surface)
+	{
+		return r;
+	}
+	r.position = reconstructWorldPosition(P, uv, depth);
+	r.normal = g.decode(uv);
+	const V4 albedoRoughness = loadU8(g.albedoTex, g.full(uv));
+	const float metallic = loadU8(g.normalTex, g.full(uv)).w;
+	r.roughness = fmaxf(albedoRoughness.w, 0.02f);
+	r.alpha = r.roughness * r.roughness;
+	const V3 camera = v3(P.camera_position[0], P.camera_position[1], P.camera_position[2]);
+	r.viewDirection = normalize(camera - r.position);
+	r.normalView = fmaxf(dot(r.normal, r.viewDirection), 0.001f);
+	r.f0 = mix(v3s(0.04f), albedoRoughness.xyz(), metallic);
+	const V2 pixel = v2(floorf(uv.x * g.giSize.x), floorf(uv.y * g.giSize.y));
+	uint32_t rng = pcg(uint32_t(pixel.x) + pcg(uint32_t(pixel.y) + pcg(uint32_t(P.frame_index) ^ 0x2545f491u)));
+
+	V3 tangent, bitangent;
+	tangentFrame(r.normal, tangent, bitangent);
+	const V3 localView = v3(dot(r.viewDirection, tangent), dot(r.viewDirection, bitangent), r.normalView);
+	const float random0 = nextRandom(rng);
+	const float random1 = nextRandom(rng);
+	const V3 localHalfway = sampleVisibleNormal(localView, r.alpha, random0, random1);
+	r.halfway = tangent * localHalfway.x + bitangent * localHalfway.y + r.normal * localHalfway.z;
+	const V3 incident = -r.viewDirection;
+	r.direction = incident - r.halfway * (2.0f * dot(r.halfway, incident));
+	r.normalLight = dot(r.normal, r.direction);
+	r.origin = r.position + r.normal * g.kRayBias();
+	return r;
+}
+
+// The hit of a BVH ray of the pass: the triangle, or the sky when enabled.
+__device__ __forceinline__ bool specularBvhHit(const GiPass& g, const SpecularRay& r, int triangleIndex, float hitDistance,
+	V3& hitPosition, float& hitId)
+{
+	if (triangleIndex >= 0)
+	{
+		hitPosition = r.origin + r.direction * hitDistance;
+		hitId = g.encodeSampleId(triangleIndex, r.direction);
+		return true;
+	}
+	if (skyEnabled(g.P))
+	{
+		hitId = kSkySampleId;
+		return true;
+	}
+	return false;
+}
+
+// fs_specular.sc:160-226 from the ray's hit: radiance, demodulation by the
+// split-sum albedo, the outlier clamp and the reprojected history.
+__device__ inline void specularFinish(const GiPass& g, const SpecularRay& r, bool hit, V3 hitPosition, float hitId,
+	const uint16_t* __restrict__ previousHdr, const uint16_t* __restrict__ specularHistory, uint16_t* out, int i)
+{
+	const RestirParams& P = g.P;
+	V3 estimate = v3s(0.0f);
+	if (hit)
+	{
+		const V3 fresnel = fresnelSchlick(r.halfway, r.viewDirection, r.f0);
+		estimate = specularHitRadiance(g, previousHdr, hitPosition, hitId, r.direction) * fresnel * smithG1(r.normalLight, r.alpha);
+	}
+	V3 demodulated = estimate / vmax(specularAlbedo(r.f0, r.roughness, r.normalView), v3s(0.001f));
+	if (P.outlier_clamp > 0.0f)
+	{
+		demodulated = vmin(demodulated, v3s(P.outlier_clamp));
+	}
+
+	V3 history = v3s(0.0f);
+	float historyLength = 0.0f;
+	const V4 clipPrevious = mul(P.prev_view_proj, v4(r.position, 1.0f));
+	if (P.history_valid > 0.5f && clipPrevious.w > 0.0001f)
+	{
+		const V2 projected = clipToUv(P, clipPrevious);
+		const V2 previousUv = v2((floorf(projected.x * g.giSize.x) + 0.5f) * g.giTexel.x,
+			(floorf(projected.y * g.giSize.y) + 0.5f) * g.giTexel.y);
+		const int h = g.gi(previousUv);
+		const float4 rp = __ldg(g.historyReceiver + h);
+		const float4 rn = __ldg(g.historyNormal + h);
+		const V3 receiverPosition = v3(rp.x, rp.y, rp.z);
+		const V3 receiverNormal = v3(rn.x, rn.y, rn.z);
+		const V3 offset = receiverPosition - r.position;
+		if (isOnScreen(previousUv) && dot(receiverNormal, receiverNormal) > 0.5f
+			&& dot(offset, offset) <= g.kBounceRadius() * g.kBounceRadius() && fabsf(dot(offset, r.normal)) <= g.kReceiverPlane()
+			&& dot(normalize(receiverNormal), r.normal) >= 0.9f)
+		{
+			const V4 previous = loadH4(specularHistory, h);
+			history = previous.xyz();
+			historyLength = previous.w;
+		}
+	}
+	const float maxHistory = mixf(4.0f, 32.0f, clampf(r.roughness * 1.5f, 0.0f, 1.0f));
+	historyLength = fminf(historyLength + 1.0f, maxHistory);
+	storeH4(out, i, v4(mix(history, demodulated, 1.0f / historyLength), historyLength));
+}
+
 // fs_specular.sc:127-226, one thread per GI pixel in 16x8 tiles.
 __global__ void __launch_bounds__(128, RESTIR_SPECULAR_MIN_BLOCKS) giSpecularKernel(const RestirParams P, BvhView bvh, GiBindings b,
 	const uint16_t* __restrict__ previousHdr, const uint16_t* __restrict__ specularHistory, uint16_t* out)
@@ -744,103 +853,112 @@ __global__ void __launch_bounds__(128, RESTIR_SPECULAR_MIN_BLOCKS) giSpecularKer
 		return;
 	}
 	const int i = py * g.w + px;
-	const V2 uv = pixelUv(px, py, g.giTexel);
-	const float depth = g.depthAt(uv);
-	if (depth >= kSkyDepth)
+	const SpecularRay r = specularRay(g, pixelUv(px, py, g.giTexel));
+	if (!r.surface)
 	{
 		storeH4(out, i, v4(0.0f, 0.0f, 0.0f, 0.0f));
 		return;
 	}
-	const V3 position = reconstructWorldPosition(P, uv, depth);
-	const V3 normal = g.decode(uv);
-	const V4 albedoRoughness = loadU8(g.albedoTex, g.full(uv));
-	const float metallic = loadU8(g.normalTex, g.full(uv)).w;
-	const float roughness = fmaxf(albedoRoughness.w, 0.02f);
-	const float alpha = roughness * roughness;
-	const V3 camera = v3(P.camera_position[0], P.camera_position[1], P.camera_position[2]);
-	const V3 viewDirection = normalize(camera - position);
-	const float normalView = fmaxf(dot(normal, viewDirection), 0.001f);
-	const V3 f0 = mix(v3s(0.04f), albedoRoughness.xyz(), metallic);
-	const V2 pixel = v2(floorf(uv.x * g.giSize.x), floorf(uv.y * g.giSize.y));
-	uint32_t rng = pcg(uint32_t(pixel.x) + pcg(uint32_t(pixel.y) + pcg(uint32_t(P.frame_index) ^ 0x2545f491u)));
-
-	V3 tangent, bitangent;
-	tangentFrame(normal, tangent, bitangent);
-	const V3 localView = v3(dot(viewDirection, tangent), dot(viewDirection, bitangent), normalView);
-	const float random0 = nextRandom(rng);
-	const float random1 = nextRandom(rng);
-	const V3 localHalfway = sampleVisibleNormal(localView, alpha, random0, random1);
-	const V3 halfway = tangent * localHalfway.x + bitangent * localHalfway.y + normal * localHalfway.z;
-	const V3 incident = -viewDirection;
-	const V3 direction = incident - halfway * (2.0f * dot(halfway, incident));
-	const float normalLight = dot(normal, direction);
-
-	V3 estimate = v3s(0.0f);
-	if (normalLight > 0.0f)
+	V3 hitPosition = v3s(0.0f);
+	float hitId = 0.0f;
+	bool hit = false;
+	if (r.normalLight > 0.0f)
 	{
-		const V3 rayOrigin = position + normal * g.kRayBias();
-		V3 hitPosition = v3s(0.0f);
-		float hitId = 0.0f;
-		bool hit = false;
 		if (P.ray_mode != RESTIR_RAY_MODE_BVH)
 		{
-			hit = g.traceScreenSpaceRay(rayOrigin, direction, g.kMaxRayDistance(), hitPosition);
+			hit = g.traceScreenSpaceRay(r.origin, r.direction, g.kMaxRayDistance(), hitPosition);
 		}
 		if (!hit && P.ray_mode != RESTIR_RAY_MODE_SCREEN)
 		{
 			float hitDistance = 0.0f;
 			// A fragment shader: no shared-memory stack, the stackless walk (bvh.sh:298-319).
-			const int triangleIndex = traceBvh(g.bvh, rayOrigin, direction, g.kMaxBvhRayDistance(), false, hitDistance, nullptr, 0);
-			if (triangleIndex >= 0)
-			{
-				hit = true;
-				hitPosition = rayOrigin + direction * hitDistance;
-				hitId = g.encodeSampleId(triangleIndex, direction);
-			}
-			else if (skyEnabled(P))
-			{
-				hit = true;
-				hitId = kSkySampleId;
-			}
-		}
-		if (hit)
-		{
-			const V3 fresnel = fresnelSchlick(halfway, viewDirection, f0);
-			estimate = specularHitRadiance(g, previousHdr, hitPosition, hitId, direction) * fresnel * smithG1(normalLight, alpha);
+			const int triangleIndex = traceBvh(g.bvh, r.origin, r.direction, g.kMaxBvhRayDistance(), false, hitDistance, nullptr, 0);
+			hit = specularBvhHit(g, r, triangleIndex, hitDistance, hitPosition, hitId);
 		}
 	}
-	V3 demodulated = estimate / vmax(specularAlbedo(f0, roughness, normalView), v3s(0.001f));
-	if (P.outlier_clamp > 0.0f)
-	{
-		demodulated = vmin(demodulated, v3s(P.outlier_clamp));
-	}
+	specularFinish(g, r, hit, hitPosition, hitId, previousHdr, specularHistory, out, i);
+}
 
-	V3 history = v3s(0.0f);
-	float historyLength = 0.0f;
-	const V4 clipPrevious = mul(P.prev_view_proj, v4(position, 1.0f));
-	if (P.history_valid > 0.5f && clipPrevious.w > 0.0001f)
+// The pass as a wavefront (restir_gi_specular_wavefront), step 1: rays and
+// depth-buffer marches; the rays the march does not answer go to the queue.
+// records[i] = (screen-space hit position, tag): tag (the float's bits) -1 no
+// hit, -2 the march's hit, else the ray's queue slot.
+__global__ void __launch_bounds__(128) specularRaysKernel(const RestirParams P, BvhView bvh, GiBindings b, float4* records,
+	RayQueue queue)
+{
+	GiPass g = makePass(P, bvh, b, P.camera_position, nullptr, 0);
+	const int px = int(blockIdx.x * 16 + threadIdx.x % 16);
+	const int py = int(blockIdx.y * 8 + threadIdx.x / 16);
+	const bool inside = px < g.w && py < g.h;
+	SpecularRay r = {};
+	V3 hitPosition = v3s(0.0f);
+	int tag = -1;
+	bool push = false;
+	if (inside)
 	{
-		const V2 projected = clipToUv(P, clipPrevious);
-		const V2 previousUv = v2((floorf(projected.x * g.giSize.x) + 0.5f) * g.giTexel.x,
-			(floorf(projected.y * g.giSize.y) + 0.5f) * g.giTexel.y);
-		const int h = g.gi(previousUv);
-		const float4 rp = __ldg(g.historyReceiver + h);
-		const float4 rn = __ldg(g.historyNormal + h);
-		const V3 receiverPosition = v3(rp.x, rp.y, rp.z);
-		const V3 receiverNormal = v3(rn.x, rn.y, rn.z);
-		const V3 offset = receiverPosition - position;
-		if (isOnScreen(previousUv) && dot(receiverNormal, receiverNormal) > 0.5f
-			&& dot(offset, offset) <= g.kBounceRadius() * g.kBounceRadius() && fabsf(dot(offset, normal)) <= g.kReceiverPlane()
-			&& dot(normalize(receiverNormal), normal) >= 0.9f)
+		r = specularRay(g, pixelUv(px, py, g.giTexel));
+		if (r.surface && r.normalLight > 0.0f)
 		{
-			const V4 previous = loadH4(specularHistory, h);
-			history = previous.xyz();
-			historyLength = previous.w;
+			bool hit = false;
+			if (P.ray_mode != RESTIR_RAY_MODE_BVH)
+			{
+				hit = g.traceScreenSpaceRay(r.origin, r.direction, g.kMaxRayDistance(), hitPosition);
+			}
+			tag = hit ? -2 : -1;
+			push = !hit && P.ray_mode != RESTIR_RAY_MODE_SCREEN;
 		}
 	}
-	const float maxHistory = mixf(4.0f, 32.0f, clampf(roughness * 1.5f, 0.0f, 1.0f));
-	historyLength = fminf(historyLength + 1.0f, maxHistory);
-	storeH4(out, i, v4(mix(history, demodulated, 1.0f / historyLength), historyLength));
+	// Every lane votes in the push, pixels outside the image included.
+	const int slot = queuePush(queue, push, r.origin, g.kMaxBvhRayDistance(), r.direction);
+	if (inside)
+	{
+		records[py * g.w + px] = make_float4(hitPosition.x, hitPosition.y, hitPosition.z, __int_as_float(push ? slot : tag));
+	}
+}
+
+// Step 3: the rest of the pass from the recorded hits, replaying step 1's
+// ray (the same two random numbers), so every value is giSpecularKernel's.
+__global__ void __launch_bounds__(128, RESTIR_SPECULAR_MIN_BLOCKS) specularShadeKernel(const RestirParams P, BvhView bvh,
+	GiBindings b, const float4* __restrict__ records, RayQueue queue, const uint16_t* __restrict__ previousHdr,
+	const uint16_t* __restrict__ specularHistory, uint16_t* out)
+{
+	GiPass g = makePass(P, bvh, b, P.camera_position, nullptr, 0);
+	const int px = int(blockIdx.x * 16 + threadIdx.x % 16);
+	const int py = int(blockIdx.y * 8 + threadIdx.x / 16);
+	if (px >= g.w || py >= g.h)
+	{
+		return;
+	}
+	const int i = py * g.w + px;
+	const SpecularRay r = specularRay(g, pixelUv(px, py, g.giTexel));
+	if (!r.surface)
+	{
+		storeH4(out, i, v4(0.0f, 0.0f, 0.0f, 0.0f));
+		return;
+	}
+	V3 hitPosition = v3s(0.0f);
+	float hitId = 0.0f;
+	bool hit = false;
+	if (r.normalLight > 0.0f)
+	{
+		const float4 record = __ldg(records + i);
+		const int tag = __float_as_int(record.w);
+		if (tag == -2)
+		{
+			hit = true;
+			hitPosition = v3(record.x, record.y, record.z);
+		}
+		else if (tag >= 0)
+		{
+			hit = specularBvhHit(g, r, queue.hitTriangle[tag], queue.hitDistance[tag], hitPosition, hitId);
+		}
+	}
+	specularFinish(g, r, hit, hitPosition, hitId, previousHdr, specularHistory, out, i);
+}
+
+__global__ void __launch_bounds__(128) traceQueueWalkKernel(BvhView bvh, RayQueue queue)
+{
+	traceQueueClosest<128, true>(bvh, queue, nullptr);
 }
 
 GiBindings bindings(const RestirGBuffer* gb, const RestirGiHistory* history, const uint32_t* grid, const float* shadowAtlas,
@@ -933,6 +1051,7 @@ extern "C" int restir_gi_specular(const RestirParams* params, const RestirScene*
 	return launchStatus();
 }
 
+
 namespace restir
 {
 namespace
@@ -1015,24 +1134,74 @@ TemporalWorkspace layoutTemporalWorkspace(const RestirParams* p, void* base)
 	return w;
 }
 
-// One resident grid of the queue tracer: SMs x blocks that fit on one SM.
+// One resident grid of a queue tracer of 128 threads per block: SMs x blocks
+// that fit on one SM.
+int residentBlocks(const void* kernel)
+{
+	int device = 0, sms = 148, perSm = 0;
+	if (cudaGetDevice(&device) == cudaSuccess)
+	{
+		cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+	}
+	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, 128, 0) != cudaSuccess || perSm < 1)
+	{
+		perSm = 1;
+	}
+	return sms * perSm;
+}
+
 int persistentBlocks()
 {
 	static int blocks = 0;
 	if (blocks == 0)
 	{
-		int device = 0, sms = 148, perSm = 0;
-		if (cudaGetDevice(&device) == cudaSuccess)
-		{
-			cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-		}
-		if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, traceQueueKernel, 128, 0) != cudaSuccess || perSm < 1)
-		{
-			perSm = 1;
-		}
-		blocks = sms * perSm;
+		blocks = residentBlocks(reinterpret_cast<const void*>(traceQueueKernel));
 	}
 	return blocks;
+}
+
+int walkBlocks()
+{
+	static int blocks = 0;
+	if (blocks == 0)
+	{
+		blocks = residentBlocks(reinterpret_cast<const void*>(traceQueueWalkKernel));
+	}
+	return blocks;
+}
+
+// The specular wavefront's workspace: [2 counters][rays 32 B x n][hit triangles
+// 4 B x n][hit distances 4 B x n][records 16 B x n], each region starting on 256
+// bytes; n = GI pixels.
+struct SpecularWorkspace
+{
+	RayQueue queue;
+	float4* records;
+	uint64_t bytes;
+};
+
+SpecularWorkspace layoutSpecularWorkspace(const RestirParams* p, void* base)
+{
+	const uint64_t n = uint64_t(p->gi_width) * p->gi_height;
+	char* at = static_cast<char*>(base);
+	uint64_t offset = 0;
+	auto region = [&](uint64_t bytes) -> char*
+	{
+		char* start = at + offset;
+		offset += (bytes + 255u) & ~uint64_t(255u);
+		return start;
+	};
+	SpecularWorkspace w = {};
+	uint32_t* counters = reinterpret_cast<uint32_t*>(region(2 * sizeof(uint32_t)));
+	w.queue.count = counters;
+	w.queue.claimed = counters + 1;
+	w.queue.rays = reinterpret_cast<float4*>(region(n * 32));
+	w.queue.hitTriangle = reinterpret_cast<int*>(region(n * 4));
+	w.queue.hitDistance = reinterpret_cast<float*>(region(n * 4));
+	w.records = reinterpret_cast<float4*>(region(n * 16));
+	w.queue.capacity = uint32_t(n);
+	w.bytes = offset;
+	return w;
 }
 
 } // namespace
@@ -1074,6 +1243,43 @@ extern "C" int restir_gi_temporal_wavefront(const RestirParams* params, const Re
 	giCandidatesKernel<<<blocks, kGiThreads, 0, s>>>(*params, bvh, b, w.records, w.queue);
 	traceQueueKernel<<<persistentBlocks(), 128, 0, s>>>(bvh, w.queue);
 	giTemporalShadeKernel<<<blocks, kGiThreads, 0, s>>>(*params, bvh, b, w.records, w.queue);
+	return launchStatus();
+}
+
+extern "C" uint64_t restir_gi_specular_workspace_bytes(const RestirParams* params)
+{
+	if (params == nullptr)
+	{
+		return 0;
+	}
+	return layoutSpecularWorkspace(params, nullptr).bytes;
+}
+
+extern "C" int restir_gi_specular_wavefront(const RestirParams* params, const RestirScene* scene, const RestirGBuffer* gbuffer,
+	const RestirGiHistory* history, const float* shadow_atlas, const uint16_t* surface_light, const uint16_t* previous_hdr,
+	const uint16_t* specular_history, uint16_t* specular, void* workspace, uint64_t workspace_bytes, void* stream)
+{
+	if (params == nullptr || scene == nullptr || gbuffer == nullptr || history == nullptr || shadow_atlas == nullptr
+		|| gbuffer->albedo == nullptr || gbuffer->normal == nullptr || gbuffer->depth == nullptr || history->receiver == nullptr
+		|| history->normal == nullptr || history->color == nullptr || previous_hdr == nullptr || specular_history == nullptr
+		|| specular == nullptr || specular == specular_history || params->gi_width == 0 || params->gi_height == 0
+		|| params->trace_steps <= 0 || workspace == nullptr || (reinterpret_cast<uintptr_t>(workspace) & 255u) != 0u)
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	SpecularWorkspace w = layoutSpecularWorkspace(params, workspace);
+	if (workspace_bytes < w.bytes)
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	GiBindings b = bindings(gbuffer, history, nullptr, shadow_atlas, surface_light);
+	const BvhView bvh = makeBvhView(scene);
+	cudaStream_t s = asStream(stream);
+	dim3 grid((params->gi_width + 15) / 16, (params->gi_height + 7) / 8);
+	cudaMemsetAsync(workspace, 0, 2 * sizeof(uint32_t), s);
+	specularRaysKernel<<<grid, 128, 0, s>>>(*params, bvh, b, w.records, w.queue);
+	traceQueueWalkKernel<<<walkBlocks(), 128, 0, s>>>(bvh, w.queue);
+	specularShadeKernel<<<grid, 128, 0, s>>>(*params, bvh, b, w.records, w.queue, previous_hdr, specular_history, specular);
 	return launchStatus();
 }
 

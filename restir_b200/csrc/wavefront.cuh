@@ -12,7 +12,9 @@
 // The per-ray algorithm is the reference's nearest-first short-stack
 // traversal (bvh.sh:216-295) written as a resumable state machine: the same
 // nodes in the same order, the same step cap, the same stackless fallback,
-// so hit ids and distances are identical to traceShortStack's.
+// so hit ids and distances are identical to traceShortStack's. The tracer's
+// walk form runs the stackless walk (bvh.sh:140-174) the same way, for the
+// rays of the fragment-shader passes.
 #pragma once
 
 #include "bvh.cuh"
@@ -98,6 +100,25 @@ __device__ __forceinline__ void startShortStack(ShortStackState& s, const BvhVie
 	}
 }
 
+// A ray of the stackless walk alone (the fragment-shader passes): phase 1
+// from the root, whose box the walk tests in its first step.
+__device__ __forceinline__ void startStacklessWalk(ShortStackState& s, V3 o, V3 d, float tmax)
+{
+	s.o = o;
+	s.d = d;
+	s.inv = bvhInverseDirection(d);
+	s.distance = tmax;
+	s.hit = -1;
+	s.fallbackHit = -1;
+	s.node = 0;
+	s.stackTop = 0;
+	s.stackCount = 0;
+	s.step = 0;
+	s.dropped = false;
+	s.work = TraceWork();
+	s.phase = 1;
+}
+
 // The end of the short-stack walk: the stackless re-walk if entries were dropped.
 __device__ __forceinline__ void endShortStack(ShortStackState& s)
 {
@@ -115,6 +136,41 @@ __device__ __forceinline__ void endShortStack(ShortStackState& s)
 	{
 		s.phase = 2;
 	}
+}
+
+// traceStacklessWalk (bvh.sh:140-174), one node per call: the short stack's
+// re-walk (phase 1), or a whole ray started by startStacklessWalk.
+__device__ __forceinline__ void stepStacklessWalk(ShortStackState& s, const BvhView& b)
+{
+	// traceStacklessWalk, one node per call.
+	if (s.step >= kBvhMaxSteps || s.node >= b.nodeCount)
+	{
+		if (s.step >= kBvhMaxSteps)
+		{
+			raiseStatus(1u);
+		}
+		if (s.fallbackHit >= 0)
+		{
+			s.hit = s.fallbackHit;
+		}
+		s.phase = 2;
+		return;
+	}
+	++s.work.nodes;
+	V4 node0 = b.row(s.node * 2);
+	V4 node1 = b.row(s.node * 2 + 1);
+	bool leaf = node1.w >= 0.0f;
+	++s.step;
+	if (intersectBox(s.o, s.inv, node0.xyz(), node1.xyz(), s.distance) < 0.0f)
+	{
+		s.node = leaf ? s.node + 1 : int(-node1.w) - 1;
+		return;
+	}
+	if (leaf)
+	{
+		s.fallbackHit = intersectLeaf(b, s.o, s.d, int(node0.w), int(node1.w), s.distance, s.fallbackHit, s.work);
+	}
+	s.node = s.node + 1;
 }
 
 // Advances the traversal by one node.
@@ -179,45 +235,19 @@ __device__ __forceinline__ void stepShortStack(ShortStackState& s, const BvhView
 	}
 	if (s.phase == 1)
 	{
-		// traceStacklessWalk, one node per call.
-		if (s.step >= kBvhMaxSteps || s.node >= b.nodeCount)
-		{
-			if (s.step >= kBvhMaxSteps)
-			{
-				raiseStatus(1u);
-			}
-			if (s.fallbackHit >= 0)
-			{
-				s.hit = s.fallbackHit;
-			}
-			s.phase = 2;
-			return;
-		}
-		++s.work.nodes;
-		V4 node0 = b.row(s.node * 2);
-		V4 node1 = b.row(s.node * 2 + 1);
-		bool leaf = node1.w >= 0.0f;
-		++s.step;
-		if (intersectBox(s.o, s.inv, node0.xyz(), node1.xyz(), s.distance) < 0.0f)
-		{
-			s.node = leaf ? s.node + 1 : int(-node1.w) - 1;
-			return;
-		}
-		if (leaf)
-		{
-			s.fallbackHit = intersectLeaf(b, s.o, s.d, int(node0.w), int(node1.w), s.distance, s.fallbackHit, s.work);
-		}
-		s.node = s.node + 1;
+		stepStacklessWalk(s, b);
 	}
 }
 
 // The persistent closest-hit tracer over a queue. Launch with a whole number
 // of warps per block; stack: kBvhShortStack ints per thread of the block.
-template<int kThreads>
+// kWalk: every ray takes the stackless walk instead (traceBvh without a
+// stack, the fragment-shader passes; no stack storage).
+template<int kThreads, bool kWalk = false>
 __device__ inline void traceQueueClosest(const BvhView& b, const RayQueue& q, int* stackStorage)
 {
 	const unsigned lane = threadIdx.x & 31u;
-	int* stack = stackStorage + threadIdx.x;
+	int* stack = kWalk ? nullptr : stackStorage + threadIdx.x;
 	const uint32_t total = q.count != nullptr ? min(*q.count, q.capacity) : q.capacity;
 	ShortStackState s;
 	s.phase = 2;
@@ -244,7 +274,14 @@ __device__ inline void traceQueueClosest(const BvhView& b, const RayQueue& q, in
 					ray = int(index);
 					float4 a = q.rays[2 * index];
 					float4 c = q.rays[2 * index + 1];
-					startShortStack(s, b, v3(a.x, a.y, a.z), v3(c.x, c.y, c.z), a.w);
+					if (kWalk)
+					{
+						startStacklessWalk(s, v3(a.x, a.y, a.z), v3(c.x, c.y, c.z), a.w);
+					}
+					else
+					{
+						startShortStack(s, b, v3(a.x, a.y, a.z), v3(c.x, c.y, c.z), a.w);
+					}
 				}
 				else
 				{
@@ -260,13 +297,20 @@ __device__ inline void traceQueueClosest(const BvhView& b, const RayQueue& q, in
 		{
 			if (s.phase != 2)
 			{
-				stepShortStack(s, b, stack, kThreads);
+				if (kWalk)
+				{
+					stepStacklessWalk(s, b);
+				}
+				else
+				{
+					stepShortStack(s, b, stack, kThreads);
+				}
 			}
 			if (s.phase == 2)
 			{
 				q.hitTriangle[ray] = s.hit;
 				q.hitDistance[ray] = s.distance;
-				countWork(RESTIR_COUNT_CLOSEST, s.work.nodes, s.work.triangles);
+				countWork(kWalk ? RESTIR_COUNT_ANY : RESTIR_COUNT_CLOSEST, s.work.nodes, s.work.triangles);
 				ray = -1;
 			}
 		}

@@ -648,12 +648,23 @@ private:
 		return RESTIR_OK;
 	}
 
-	// The wavefront GI temporal pass's ray queue, sized by the candidate count
-	// (a setting that keeps the history); allocated before any capture.
+	// The wavefront passes' ray queues: GI temporal's, sized by the candidate
+	// count (a setting that keeps the history), and the specular pass's;
+	// allocated before any capture.
 	int ensureWorkspace(const RestirParams& P)
 	{
-		const uint64_t needed = m_settings.wavefront ? restir_gi_temporal_workspace_bytes(&P) : 0;
-		auto found = m_targets.find("gi.workspace");
+		const int status = ensureBuffer("gi.workspace", m_settings.wavefront ? restir_gi_temporal_workspace_bytes(&P) : 0);
+		if (status != RESTIR_OK)
+		{
+			return status;
+		}
+		return ensureBuffer("specular.workspace",
+			m_settings.wavefront && m_settings.specular_gi ? restir_gi_specular_workspace_bytes(&P) : 0);
+	}
+
+	int ensureBuffer(const char* name, uint64_t needed)
+	{
+		auto found = m_targets.find(name);
 		if (needed == 0 || (found != m_targets.end() && found->second.bytes >= needed))
 		{
 			return RESTIR_OK;
@@ -671,7 +682,7 @@ private:
 		{
 			return RESTIR_ERROR_OUT_OF_MEMORY;
 		}
-		m_targets["gi.workspace"] = b;
+		m_targets[name] = b;
 		return RESTIR_OK;
 	}
 
@@ -863,6 +874,12 @@ private:
 		{
 			// Indirect specular (renderer.cpp:835-855): last frame's composite and specular history.
 			run(RESTIR_PASS_SPECULAR, [&] {
+				if (m_settings.wavefront)
+				{
+					const Buffer& w = m_targets["specular.workspace"];
+					return restir_gi_specular_wavefront(&P, &scene, &gb, &history, atlas, surface, p<uint16_t>("hdr"),
+						p<uint16_t>(specularRead), p<uint16_t>(specularWrite), w.pointer, w.bytes, s);
+				}
 				return restir_gi_specular(&P, &scene, &gb, &history, atlas, surface, p<uint16_t>("hdr"),
 					p<uint16_t>(specularRead), p<uint16_t>(specularWrite), s);
 			});

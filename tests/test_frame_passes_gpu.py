@@ -63,8 +63,9 @@ def test_frame_passes_bit_exact(case):
 @pytest.mark.gpu
 @pytest.mark.parametrize("case", list(CASES))
 def test_gi_temporal_wavefront_bit_exact(case):
-    """The wavefront GI temporal pass (candidates, queued tracer, shading)
-    reproduces the oracle's reservoirs bit for bit, like the single-kernel pass."""
+    """The wavefront GI temporal pass (candidates, queued tracer, shading) and
+    the wavefront specular pass (rays, queued stackless walk, shading)
+    reproduce the oracle's outputs bit for bit, like the single-kernel passes."""
     c, setup, settings = _case_setup(case)
     w, h = c["size"]
     rb.status_flags()
@@ -132,6 +133,53 @@ def test_gi_temporal_wavefront_rejects_bad_workspace():
     assert lib.restir_gi_temporal_wavefront(*args, space.data_ptr(), nbytes - 1, None) == rb.ERROR_INVALID_ARGUMENT
     assert lib.restir_gi_temporal_wavefront(*args, None, nbytes, None) == rb.ERROR_INVALID_ARGUMENT
     torch.cuda.synchronize()
+
+
+@pytest.mark.gpu
+def test_gi_specular_wavefront_rejects_bad_workspace():
+    import torch
+    setup = make_scene(rb.SCENE_CORNELL)
+    runner = FrameRunner(setup, 32, 32, "cuda", gi_wavefront=True)
+    P, _ = runner.prepare()
+    lib = runner.lib
+    nbytes = int(lib.restir_gi_specular_workspace_bytes(P))
+    n = P.gi_width * P.gi_height
+    assert nbytes == 256 + sum((b * n + 255) // 256 * 256 for b in (32, 4, 4, 16))
+    space = torch.zeros(nbytes + 256, dtype=torch.uint8, device="cuda")
+    from restir_b200.abi import RestirGiHistory
+    hist = RestirGiHistory(runner.b("gi.sample0"), runner.b("gi.receiver0"), runner.b("gi.normal0"),
+                           runner.b("gi.color0"), runner.b("gi.moments0"))
+    args = (P, runner.scene, runner.gbuffer(), hist, runner.b("atlas"), runner.b("gb.emissive"), runner.b("hdr"),
+            runner.b("specular0"), runner.b("specular1"))
+    # Misaligned, too small, missing.
+    assert lib.restir_gi_specular_wavefront(*args, space.data_ptr() + 16, nbytes, None) == rb.ERROR_INVALID_ARGUMENT
+    assert lib.restir_gi_specular_wavefront(*args, space.data_ptr(), nbytes - 1, None) == rb.ERROR_INVALID_ARGUMENT
+    assert lib.restir_gi_specular_wavefront(*args, None, nbytes, None) == rb.ERROR_INVALID_ARGUMENT
+    assert lib.restir_gi_specular_wavefront(*args, space.data_ptr(), nbytes, None) == rb.OK
+    torch.cuda.synchronize()
+
+
+@pytest.mark.gpu
+def test_renderer_wavefront_frames_equal_single_kernel_frames():
+    """The renderer's wavefront passes (GI temporal and specular through ray
+    queues) give the single-kernel frames bit for bit on a 100k-triangle
+    scene with sky, over frames that carry history."""
+    mesh = rb.Mesh.procedural(rb.SCENE_COURTYARD, 2, 100000)
+    frames = {}
+    for wavefront in (0, 1):
+        settings = rb.default_settings(mesh)
+        settings.wavefront = wavefront
+        settings.grid_mode = rb.GRID_DETERMINISTIC
+        renderer = rb.Renderer(settings)
+        renderer.set_scene(mesh, use_scene_defaults=False)
+        frame = rb.frame_input(mesh, 240, 136)
+        for _ in range(3):
+            renderer.render(frame)
+        frames[wavefront] = {name: renderer.download(name, np.uint16)
+                             for name in ("specular0", "specular1", "hdr", "display.hdr")}
+    for name in frames[0]:
+        np.testing.assert_array_equal(frames[0][name], frames[1][name], err_msg=name)
+    assert np.count_nonzero(frames[1]["specular0"]) + np.count_nonzero(frames[1]["specular1"]) > 0
 
 
 @pytest.mark.gpu
