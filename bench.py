@@ -590,11 +590,12 @@ def own_arm(args, rank: int, world: int) -> None:
     achieved = float(pass_bytes[passes[dominant]] / (mean_pass[dominant] * 1e-3) / 1e9) if mean_pass[dominant] > 0 else 0.0
     share = {name: (mean_pass[i] / ms_per_frame if ms_per_frame > 0 else 0.0) for i, name in enumerate(passes)}
     # shadow, G-buffer, DI x2, grid x2, GI temporal (3 kernels as a wavefront), GI spatial, denoiser, composite,
-    # display (auto exposure when on, then TAA + tone mapping)
+    # display (auto exposure when on, then TAA + tone mapping), specular (3 kernels as a wavefront)
     gi_temporal_kernels = 3 if settings.wavefront else 1
     launches = (2 + (2 if plan.di_active else 0) + 2 + gi_temporal_kernels + 1
                 + (1 + plan.atrous_iterations if plan.denoiser else 0) + 1
-                + ((1 + plan.exposure) if plan.display else 0) + (1 if plan.specular else 0))
+                + ((1 + plan.exposure) if plan.display else 0)
+                + ((3 if settings.wavefront else 1) if plan.specular else 0))
 
     baseline = cpu_baseline(steps=1, scale=2) if not args.no_cpu_baseline else None
     line = {

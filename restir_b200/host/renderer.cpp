@@ -81,6 +81,10 @@ public:
 		cudaStreamCreateWithFlags(&m_side, cudaStreamNonBlocking);
 		cudaEventCreateWithFlags(&m_fork, cudaEventDisableTiming);
 		cudaEventCreateWithFlags(&m_join, cudaEventDisableTiming);
+		cudaStreamCreateWithFlags(&m_aside, cudaStreamNonBlocking);
+		cudaEventCreateWithFlags(&m_asideFork, cudaEventDisableTiming);
+		cudaEventCreateWithFlags(&m_shadowJoin, cudaEventDisableTiming);
+		cudaEventCreateWithFlags(&m_specularJoin, cudaEventDisableTiming);
 		for (auto& frame : m_events)
 		{
 			for (auto& pass : frame)
@@ -111,6 +115,11 @@ public:
 		cudaEventDestroy(m_fork);
 		cudaEventDestroy(m_join);
 		cudaStreamDestroy(m_side);
+		cudaStreamSynchronize(m_aside);
+		cudaEventDestroy(m_asideFork);
+		cudaEventDestroy(m_shadowJoin);
+		cudaEventDestroy(m_specularJoin);
+		cudaStreamDestroy(m_aside);
 		cudaStreamDestroy(m_stream);
 	}
 
@@ -748,11 +757,52 @@ private:
 				}
 			}
 		};
+		// Two passes run on a second stream beside the main chain: the shadow
+		// atlas (first read by the GI passes) beside the G-buffer and the DI
+		// passes, and the specular pass (it reads last frame's GI history and
+		// this frame's DI output, nothing the GI passes or the denoiser write)
+		// beside the GI passes and the denoiser. Not in a profiling frame (its
+		// counters wait pass by pass) nor in a batch's parts.
+		const bool overlap = part == kWholeFrame && m_profile == nullptr;
+		auto runAside = [&](int pass, cudaEvent_t join, auto&& body)
+		{
+			cudaEventRecord(m_asideFork, m_stream);
+			cudaStreamWaitEvent(m_aside, m_asideFork, 0);
+			if (events)
+			{
+				cudaEventRecord(m_events[m_slot][pass][0], m_aside);
+			}
+			status |= body(static_cast<void*>(m_aside));
+			m_passRan[m_slot][pass] = true;
+			if (events)
+			{
+				cudaEventRecord(m_events[m_slot][pass][1], m_aside);
+			}
+			cudaEventRecord(join, m_aside);
+		};
+		bool shadowPending = false;
+		bool specularPending = false;
+		auto needAtlas = [&]()
+		{
+			if (shadowPending)
+			{
+				cudaStreamWaitEvent(m_stream, m_shadowJoin, 0);
+				shadowPending = false;
+			}
+		};
 		// A batch draws the shadow atlas once for all its views (it depends on the light and scene only).
 		float* atlas = m_sharedAtlas != nullptr ? m_sharedAtlas : p<float>("shadow.atlas");
 		if (before && m_sharedAtlas == nullptr)
 		{
-			run(RESTIR_PASS_SHADOW, [&] { return restir_shadow_atlas(&P, &scene, atlas, s); });
+			if (overlap)
+			{
+				runAside(RESTIR_PASS_SHADOW, m_shadowJoin, [&](void* st) { return restir_shadow_atlas(&P, &scene, atlas, st); });
+				shadowPending = true;
+			}
+			else
+			{
+				run(RESTIR_PASS_SHADOW, [&] { return restir_shadow_atlas(&P, &scene, atlas, s); });
+			}
 		}
 		if (before)
 		{
@@ -768,6 +818,7 @@ private:
 		bool joinSide = false;
 		auto train = [&]()
 		{
+			needAtlas();
 			const Buffer& w = m_targets["gi.workspace"];
 			if (m_profile != nullptr)
 			{
@@ -798,6 +849,7 @@ private:
 			// The cache-only form's GI needs only the G-buffer: its queries first,
 			// then the training overlaps the DI passes.
 			RestirGiReservoirs current = { p<float>("gi.sample" + H), p<float>("gi.receiver" + H), p<float>("gi.normal" + H) };
+			needAtlas();
 			run(RESTIR_PASS_GI_TEMPORAL, [&] {
 				const Buffer& w = m_targets["gi.workspace"];
 				return restir_gi_from_cache(&P, &scene, &gb, &m_scene->cacheConfig, cacheState, w.pointer, w.bytes, &current,
@@ -818,15 +870,35 @@ private:
 		const uint16_t* surface = plan.surface_light_is_di ? (plan.di_active ? p<uint16_t>("di.diffuse") : p<uint16_t>("black"))
 			: p<uint16_t>("gbuffer.emissive");
 		uint32_t* gridWrite = p<uint32_t>("grid" + H);
+		RestirGiHistory history = { p<float>("gi.sample" + R), p<float>("gi.receiver" + R), p<float>("gi.normal" + R),
+			plan.denoiser ? p<uint16_t>("filtered" + R) : p<uint16_t>("gi.color" + R), p<uint16_t>("gi.moments" + R) };
+		const std::string specularRead = "specular" + std::to_string(m_specularRead);
+		const std::string specularWrite = "specular" + std::to_string(1 - m_specularRead);
+		auto specular = [&](void* st)
+		{
+			if (m_settings.wavefront)
+			{
+				const Buffer& w = m_targets["specular.workspace"];
+				return restir_gi_specular_wavefront(&P, &scene, &gb, &history, atlas, surface, p<uint16_t>("hdr"),
+					p<uint16_t>(specularRead), p<uint16_t>(specularWrite), w.pointer, w.bytes, st);
+			}
+			return restir_gi_specular(&P, &scene, &gb, &history, atlas, surface, p<uint16_t>("hdr"),
+				p<uint16_t>(specularRead), p<uint16_t>(specularWrite), st);
+		};
+		if (plan.specular && overlap)
+		{
+			// Indirect specular (renderer.cpp:835-855): last frame's composite and specular history.
+			runAside(RESTIR_PASS_SPECULAR, m_specularJoin, specular);
+			specularPending = true;
+		}
 		if (before && !plan.gi_from_cache)
 		{
 			run(RESTIR_PASS_GRID, [&] {
 				return restir_grid_clear(&P, gridWrite, s) | restir_grid_insert(&P, &gb, gridWrite, s);
 			});
 		}
-		RestirGiHistory history = { p<float>("gi.sample" + R), p<float>("gi.receiver" + R), p<float>("gi.normal" + R),
-			plan.denoiser ? p<uint16_t>("filtered" + R) : p<uint16_t>("gi.color" + R), p<uint16_t>("gi.moments" + R) };
 		RestirGiReservoirs current = { p<float>("gi.sample" + H), p<float>("gi.receiver" + H), p<float>("gi.normal" + H) };
+		needAtlas();
 		if (part != kWholeFrame)
 		{
 			// The batch's shared ray queue: candidates before its one tracer launch, shading after.
@@ -868,21 +940,9 @@ private:
 			return restir_gi_spatial(&P, &scene, &gb, &current, gridWrite, &history, atlas, surface,
 				p<uint16_t>("gi.color" + H), p<uint16_t>("gi.moments" + H), s);
 		});
-		const std::string specularRead = "specular" + std::to_string(m_specularRead);
-		const std::string specularWrite = "specular" + std::to_string(1 - m_specularRead);
-		if (plan.specular)
+		if (plan.specular && !overlap)
 		{
-			// Indirect specular (renderer.cpp:835-855): last frame's composite and specular history.
-			run(RESTIR_PASS_SPECULAR, [&] {
-				if (m_settings.wavefront)
-				{
-					const Buffer& w = m_targets["specular.workspace"];
-					return restir_gi_specular_wavefront(&P, &scene, &gb, &history, atlas, surface, p<uint16_t>("hdr"),
-						p<uint16_t>(specularRead), p<uint16_t>(specularWrite), w.pointer, w.bytes, s);
-				}
-				return restir_gi_specular(&P, &scene, &gb, &history, atlas, surface, p<uint16_t>("hdr"),
-					p<uint16_t>(specularRead), p<uint16_t>(specularWrite), s);
-			});
+			run(RESTIR_PASS_SPECULAR, [&] { return specular(s); });
 		}
 		if (cached && !plan.gi_from_cache)
 		{
@@ -908,6 +968,10 @@ private:
 		}
 		const uint16_t* diDiffuse = plan.di_active ? p<uint16_t>("di.diffuse") : p<uint16_t>("black");
 		const uint16_t* diSpecular = plan.di_active ? p<uint16_t>("di.specular") : p<uint16_t>("black");
+		if (specularPending)
+		{
+			cudaStreamWaitEvent(m_stream, m_specularJoin, 0);
+		}
 		run(RESTIR_PASS_COMPOSITE, [&] {
 			return restir_composite_specular(&P, &gb, atlas, p<uint16_t>(denoised), diDiffuse, diSpecular,
 				plan.specular ? p<uint16_t>(specularWrite) : nullptr, p<uint16_t>("hdr"), s);
@@ -1030,6 +1094,8 @@ private:
 	cudaStream_t m_stream = nullptr;
 	cudaStream_t m_side = nullptr;   // the cache's training, overlapping the rest of the frame
 	cudaEvent_t m_fork = nullptr, m_join = nullptr;
+	cudaStream_t m_aside = nullptr;  // the shadow atlas and the specular pass, beside the main chain
+	cudaEvent_t m_asideFork = nullptr, m_shadowJoin = nullptr, m_specularJoin = nullptr;
 	cudaGraphExec_t m_graphExec = nullptr;
 	double* m_errorHost = nullptr;
 	uint64_t* m_profile = nullptr;
