@@ -77,7 +77,12 @@ public:
 		{
 			m_state.previous_view_proj[i * 5] = 1.0f;
 		}
-		cudaStreamCreateWithFlags(&m_stream, cudaStreamNonBlocking);
+		// The main chain of passes at the device's highest stream priority: the
+		// block scheduler then fills what it leaves free with the passes on
+		// the side streams, instead of stretching the chain.
+		int leastPriority = 0, greatestPriority = 0;
+		cudaDeviceGetStreamPriorityRange(&leastPriority, &greatestPriority);
+		cudaStreamCreateWithPriority(&m_stream, cudaStreamNonBlocking, greatestPriority);
 		cudaStreamCreateWithFlags(&m_side, cudaStreamNonBlocking);
 		cudaEventCreateWithFlags(&m_fork, cudaEventDisableTiming);
 		cudaEventCreateWithFlags(&m_join, cudaEventDisableTiming);
