@@ -50,6 +50,7 @@ ERROR_FRAMES = 240         # frames the relMSE is averaged over (it swings by +-
 # workload (profiles/gi_temporal_wavefront_1080p_city1M.md): candidates 15.9 MB, queue tracer
 # 30.7 MB, shading 83.9 MB.
 DOMINANT_TRAFFIC = {"gi_temporal": 130.5e6}
+SIDE_STREAM_PASSES = ("shadow", "specular")
 CACHE_TRAIN_FRAMES = 60    # online training before the radiance-cache form is timed
 
 # Algorithmic (compulsory) bytes per pixel of each pass's image reads and
@@ -544,6 +545,8 @@ def own_arm(args, rank: int, world: int) -> None:
     clocks = sampler.stop()
     pass_ms = renderer.pass_history(args.steps) if not args.graph else np.zeros((0, len(rb.PASS_NAMES)))
     metrics = renderer.frame_submitted()
+    # The timed frames' plan (the radiance-cache arms below change the settings).
+    params, plan, _ = renderer.last_frame()
 
     # End to end through the public API: each step renders the frame from its
     # host-side input and reads the frame's error record back to the host.
@@ -571,7 +574,6 @@ def own_arm(args, rank: int, world: int) -> None:
             dist.destroy_process_group()
         return
 
-    params, plan, _ = renderer.last_frame()
     ms_per_frame = elapsed_ms / args.steps
     rays = int(counts[:, 0:4].sum())
     passes = rb.PASS_NAMES
@@ -585,7 +587,11 @@ def own_arm(args, rank: int, world: int) -> None:
         pixel_bytes = sizes[res] * per_pixel + (8 * params.grid_table_size if name == "grid" else 0)
         pass_bytes[name] = (pixel_bytes + 32 * int(counts[i, 4]) + 48 * int(counts[i, 5])) if ran else 0
     mean_pass = [float(v) for v in mean_pass]
-    dominant = int(np.argmax(mean_pass))
+    # The dominant pass of the main chain: the shadow atlas and the specular pass
+    # run on a second, lower-priority stream, so their event intervals include
+    # the time they wait behind the chain for free SMs.
+    chain = [i for i, name in enumerate(passes) if name not in SIDE_STREAM_PASSES]
+    dominant = max(chain, key=lambda i: mean_pass[i])
     peak, peak_kind = load_peaks()
     achieved = float(pass_bytes[passes[dominant]] / (mean_pass[dominant] * 1e-3) / 1e9) if mean_pass[dominant] > 0 else 0.0
     share = {name: (mean_pass[i] / ms_per_frame if ms_per_frame > 0 else 0.0) for i, name in enumerate(passes)}
@@ -622,6 +628,7 @@ def own_arm(args, rank: int, world: int) -> None:
                                               if cache_only_line and cache_only_line["rel_mse_vs_fp64_reference"]
                                               <= plain_error["mean"] else None),
         "pass_ms": {name: float(mean_pass[i]) for i, name in enumerate(passes)},
+        "side_stream_passes": list(SIDE_STREAM_PASSES),
         "pass_share": share,
         "pass_algorithmic_gbs": {name: (float(pass_bytes[name] / (mean_pass[i] * 1e-3) / 1e9) if mean_pass[i] > 0 else 0.0)
                                  for i, name in enumerate(passes)},

@@ -516,21 +516,23 @@ struct GiPass
 		{
 			return true;
 		}
-		V3 radiance;
+		// The sample point's albedo and its own light (the surface light of a
+		// visible point, a triangle's emission otherwise), then one call site
+		// each for the light terms, which keeps the kernels that inline this small.
+		V3 albedo;
+		V3 ownLight;
 		if (visibleSurface)
 		{
-			V3 albedo = diffuseAlbedo(sampleUv);
-			radiance = directFromLight(albedo, samplePosition, sampleNormal)
-				+ sampleIndirect(samplePosition, sampleNormal, albedo, cacheSlot)
-				+ loadH4(surfaceLight, full(sampleUv)).xyz() * P.surface_light_scale;
+			albedo = diffuseAlbedo(sampleUv);
+			ownLight = loadH4(surfaceLight, full(sampleUv)).xyz() * P.surface_light_scale;
 		}
 		else
 		{
-			V3 albedo = bvh.albedo(triangleIndex);
-			radiance = directFromLight(albedo, samplePosition, sampleNormal)
-				+ sampleIndirect(samplePosition, sampleNormal, albedo, cacheSlot)
-				+ bvh.emission(triangleIndex) * P.emission_scale;
+			albedo = bvh.albedo(triangleIndex);
+			ownLight = bvh.emission(triangleIndex) * P.emission_scale;
 		}
+		const V3 radiance = directFromLight(albedo, samplePosition, sampleNormal)
+			+ sampleIndirect(samplePosition, sampleNormal, albedo, cacheSlot) + ownLight;
 		contribution = receiverAlbedo * radiance * (receiverCosine / kPi);
 		return true;
 	}
@@ -561,29 +563,21 @@ struct GiPass
 		V3 toSample = sky ? samplePosition * kMaxBvhRayDistance() : samplePosition - origin;
 		float sampleDistance = length(toSample);
 		V3 direction = toSample / fmaxf(sampleDistance, 0.0001f);
-		bool visible = true;
+		// One traversal call site for both ray kinds (a sky sample without a BVH
+		// is not visible), which keeps the kernels that inline this small.
+		const bool bvhRay = sky ? bvh.available() : P.ray_mode == RESTIR_RAY_MODE_BVH && bvh.available();
+		if (bvhRay)
+		{
+			float occluderDistance = 0.0f;
+			return traceVisibility(bvh, origin, direction, sky ? kMaxBvhRayDistance() : sampleDistance - kRayBias(),
+				occluderDistance, P.wave_visibility > 0.5f) < 0;
+		}
 		if (sky)
 		{
-			float occluderDistance = 0.0f;
-			visible = false;
-			if (bvh.available())
-			{
-				visible = traceVisibility(bvh, origin, direction, kMaxBvhRayDistance(), occluderDistance,
-					P.wave_visibility > 0.5f) < 0;
-			}
+			return false;
 		}
-		else if (P.ray_mode == RESTIR_RAY_MODE_BVH && bvh.available())
-		{
-			float occluderDistance = 0.0f;
-			visible = traceVisibility(bvh, origin, direction, sampleDistance - kRayBias(), occluderDistance,
-				P.wave_visibility > 0.5f) < 0;
-		}
-		else
-		{
-			V3 occluderPosition;
-			visible = !traceScreenSpaceRay(origin, direction, sampleDistance * 0.95f - 0.05f * s(), occluderPosition);
-		}
-		return visible;
+		V3 occluderPosition;
+		return !traceScreenSpaceRay(origin, direction, sampleDistance * 0.95f - 0.05f * s(), occluderPosition);
 	}
 
 	__device__ __forceinline__ float reconnectionJacobian(V3 here, V3 there, V3 samplePosition, V3 sampleNormal, float sampleId) const

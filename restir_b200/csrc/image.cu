@@ -134,6 +134,17 @@ __global__ void __launch_bounds__(128) atrousKernel(const RestirParams P, int st
 	const float luminanceScale = 1.0f / (4.0f * sqrtf(fmaxf(variance, 0.0f)) + 0.0001f);
 	const float stepSize = float(step);
 	const V2 spacing = v2(stepSize * texel.x, stepSize * texel.y);
+	// The taps' texel columns and rows (the coordinates are separable: a tap's
+	// u depends on x only, its v on y only), -1 outside the image.
+	int columns[5];
+	int rows[5];
+	for (int k = 0; k < 5; ++k)
+	{
+		const float u = uv.x + float(k - 2) * spacing.x;
+		const float v = uv.y + float(k - 2) * spacing.y;
+		columns[k] = u >= 0.0f && u <= 1.0f ? texelCoord(u, w) : -1;
+		rows[k] = v >= 0.0f && v <= 1.0f ? texelCoord(v, h) * w : -1;
+	}
 	V3 colorSum = v3s(0.0f);
 	float varianceSum = 0.0f;
 	float weightSum = 0.0f;
@@ -141,12 +152,11 @@ __global__ void __launch_bounds__(128) atrousKernel(const RestirParams P, int st
 	{
 		for (int x = -2; x <= 2; ++x)
 		{
-			V2 tapUv = v2(uv.x + float(x) * spacing.x, uv.y + float(y) * spacing.y);
-			if (!isInside(tapUv))
+			if (rows[y + 2] < 0 || columns[x + 2] < 0)
 			{
 				continue;
 			}
-			int j = texelIndex(tapUv, w, h);
+			int j = rows[y + 2] + columns[x + 2];
 			V4 tap = loadH4(input, j);
 			float weight = splineWeight(x) * splineWeight(y);
 			if (x != 0 || y != 0)
