@@ -49,7 +49,7 @@ ERROR_FRAMES = 240         # frames the relMSE is averaged over (it swings by +-
 # DRAM bytes (read + write) per frame of a pass's kernels, from the committed ncu capture of this
 # workload (profiles/gi_temporal_wavefront_1080p_city1M.md): candidates 15.9 MB, queue tracer
 # 30.7 MB, shading 83.9 MB.
-DOMINANT_TRAFFIC = {"gi_temporal": 130.5e6}
+DOMINANT_TRAFFIC = {"gi_temporal": 134.9e6}
 SIDE_STREAM_PASSES = ("shadow", "specular")
 CACHE_TRAIN_FRAMES = 60    # online training before the radiance-cache form is timed
 
