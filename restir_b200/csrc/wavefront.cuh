@@ -138,11 +138,15 @@ __device__ __forceinline__ void endShortStack(ShortStackState& s)
 	}
 }
 
-// traceStacklessWalk (bvh.sh:140-174), one node per call: the short stack's
-// re-walk (phase 1), or a whole ray started by startStacklessWalk.
+// traceStacklessWalk (bvh.sh:140-174), one node per call (the short stack's
+// re-walk, phase 1) or, with kPair, one or two (a whole ray started by
+// startStacklessWalk): the rows of the node after this one are fetched with
+// this node's, and when the walk goes on to it (a box passed, or a leaf) it
+// is visited in the same call, so that fetch's latency overlaps this node's
+// test. Nodes, order and step count are the walk's.
+template<bool kPair>
 __device__ __forceinline__ void stepStacklessWalk(ShortStackState& s, const BvhView& b)
 {
-	// traceStacklessWalk, one node per call.
 	if (s.step >= kBvhMaxSteps || s.node >= b.nodeCount)
 	{
 		if (s.step >= kBvhMaxSteps)
@@ -156,21 +160,37 @@ __device__ __forceinline__ void stepStacklessWalk(ShortStackState& s, const BvhV
 		s.phase = 2;
 		return;
 	}
-	++s.work.nodes;
-	V4 node0 = b.row(s.node * 2);
-	V4 node1 = b.row(s.node * 2 + 1);
-	bool leaf = node1.w >= 0.0f;
-	++s.step;
-	if (intersectBox(s.o, s.inv, node0.xyz(), node1.xyz(), s.distance) < 0.0f)
+	const int following = s.node + 1;
+	const bool fetched = kPair && following < b.nodeCount;
+	const V4 node0 = b.row(s.node * 2);
+	const V4 node1 = b.row(s.node * 2 + 1);
+	V4 next0 = node0, next1 = node1;
+	if (fetched)
 	{
-		s.node = leaf ? s.node + 1 : int(-node1.w) - 1;
-		return;
+		next0 = b.row(following * 2);
+		next1 = b.row(following * 2 + 1);
 	}
-	if (leaf)
+	auto visit = [&](const V4& row0, const V4& row1)
 	{
-		s.fallbackHit = intersectLeaf(b, s.o, s.d, int(node0.w), int(node1.w), s.distance, s.fallbackHit, s.work);
+		++s.work.nodes;
+		++s.step;
+		const bool leaf = row1.w >= 0.0f;
+		if (intersectBox(s.o, s.inv, row0.xyz(), row1.xyz(), s.distance) < 0.0f)
+		{
+			s.node = leaf ? s.node + 1 : int(-row1.w) - 1;
+			return;
+		}
+		if (leaf)
+		{
+			s.fallbackHit = intersectLeaf(b, s.o, s.d, int(row0.w), int(row1.w), s.distance, s.fallbackHit, s.work);
+		}
+		s.node = s.node + 1;
+	};
+	visit(node0, node1);
+	if (fetched && s.node == following && s.step < kBvhMaxSteps)
+	{
+		visit(next0, next1);
 	}
-	s.node = s.node + 1;
 }
 
 // Advances the traversal by one node.
@@ -235,7 +255,7 @@ __device__ __forceinline__ void stepShortStack(ShortStackState& s, const BvhView
 	}
 	if (s.phase == 1)
 	{
-		stepStacklessWalk(s, b);
+		stepStacklessWalk<false>(s, b);
 	}
 }
 
@@ -299,7 +319,7 @@ __device__ inline void traceQueueClosest(const BvhView& b, const RayQueue& q, in
 			{
 				if (kWalk)
 				{
-					stepStacklessWalk(s, b);
+					stepStacklessWalk<true>(s, b);
 				}
 				else
 				{
