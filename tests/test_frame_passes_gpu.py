@@ -183,6 +183,28 @@ def test_renderer_wavefront_frames_equal_single_kernel_frames():
 
 
 @pytest.mark.gpu
+def test_renderer_graph_frames_equal_stream_frames():
+    """Frames replayed as CUDA graphs (restir_renderer_render_graph), with the
+    side streams of the shadow atlas and the specular pass forked and joined
+    inside each capture, equal the stream-launched frames bit for bit."""
+    mesh = rb.Mesh.procedural(rb.SCENE_COURTYARD, 2, 50000)
+    frames = {}
+    for graph in (False, True):
+        settings = rb.default_settings(mesh)
+        settings.grid_mode = rb.GRID_DETERMINISTIC
+        renderer = rb.Renderer(settings)
+        renderer.set_scene(mesh, use_scene_defaults=False)
+        frame = rb.frame_input(mesh, 160, 96)
+        for _ in range(3):
+            renderer.render(frame, graph=graph)
+        frames[graph] = {name: renderer.download(name, np.uint16)
+                         for name in ("hdr", "display.hdr", "specular0", "specular1", "shadow.atlas")}
+    for name in frames[False]:
+        np.testing.assert_array_equal(frames[False][name], frames[True][name], err_msg=name)
+    assert np.count_nonzero(frames[True]["hdr"]) > 0
+
+
+@pytest.mark.gpu
 def test_reference_accumulation_and_error_fp64():
     setup = make_scene(rb.SCENE_CORNELL)
     settings = setup.settings
