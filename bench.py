@@ -48,14 +48,15 @@ REFERENCE_FRAMES = 64
 ERROR_FRAMES = 240         # frames the relMSE is averaged over (it swings by +-0.07 between 30-frame windows)
 # DRAM bytes (read + write) per frame of a pass's kernels, from the committed ncu capture of this
 # workload (profiles/gi_temporal_wavefront_1080p_city1M.md): candidates 15.9 MB, queue tracer
-# 30.7 MB, shading 83.9 MB.
+# 30.7 MB, shading 88.2 MB.
 DOMINANT_TRAFFIC = {"gi_temporal": 134.9e6}
 SIDE_STREAM_PASSES = ("shadow", "specular")
 CACHE_TRAIN_FRAMES = 60    # online training before the radiance-cache form is timed
 
 # Algorithmic (compulsory) bytes per pixel of each pass's image reads and
 # writes, besides its BVH traversal (32 B per node fetch, 48 B per triangle
-# test): see DESIGN.md, "Roofline".
+# test, counted on the device in a profiling frame): the G-buffer, reservoir,
+# history and target texels each pass must read or write once.
 PASS_PIXEL_BYTES = {
     "shadow": ("atlas", 4),
     "gbuffer": ("full", 24),
