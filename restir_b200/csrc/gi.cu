@@ -22,11 +22,13 @@ constexpr int kGiThreads = 32 * kGiWarps;
 // Minimum resident blocks per SM (register budget) of the two GI kernels.
 // Measured on the 1080p frame (launch-bound sweep): the spatial pass gains
 // from 8 blocks (64 registers, a little spilling to L1); the temporal pass is
-// bound by divergence more than occupancy: its wavefront form takes 3.00 ms
-// at its natural 150 registers (3 blocks), 2.97 / 2.96 / 2.91 ms at 4 / 5 / 6
-// blocks (6: 80 registers, 270 bytes spilled to L1).
+// bound by divergence and instruction fetch more than occupancy: its
+// wavefront form took 3.00 ms at its natural 150 registers (3 blocks) and
+// 2.91 ms at 6 blocks (80 registers); once its code was made smaller the
+// shading kernel takes 1.11 / 1.06 / 1.02 ms at 6 / 7 / 8 blocks (8: 64
+// registers, a few hundred bytes spilled to L1).
 #ifndef RESTIR_GI_TEMPORAL_MIN_BLOCKS
-#	define RESTIR_GI_TEMPORAL_MIN_BLOCKS 6
+#	define RESTIR_GI_TEMPORAL_MIN_BLOCKS 8
 #endif
 #ifndef RESTIR_GI_SPATIAL_MIN_BLOCKS
 #	define RESTIR_GI_SPATIAL_MIN_BLOCKS 8
