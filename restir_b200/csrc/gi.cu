@@ -464,7 +464,14 @@ struct CandidateRecords
 	int candidates;
 };
 
-__global__ void __launch_bounds__(kGiThreads) giCandidatesKernel(const RestirParams P, BvhView bvh, GiBindings b,
+// Minimum resident blocks per SM of the GI candidates kernel: 0.347 ms at its
+// natural 83 registers (5 blocks), 0.329 / 0.313 ms at 6 / 8 blocks (8: 64
+// registers) on the 1080p frame; its depth-buffer marches are latency-bound.
+#ifndef RESTIR_GI_CANDIDATES_MIN_BLOCKS
+#	define RESTIR_GI_CANDIDATES_MIN_BLOCKS 8
+#endif
+
+__global__ void __launch_bounds__(kGiThreads, RESTIR_GI_CANDIDATES_MIN_BLOCKS) giCandidatesKernel(const RestirParams P, BvhView bvh, GiBindings b,
 	CandidateRecords records, RayQueue queue)
 {
 	const int lane = int(threadIdx.x & 31u);
