@@ -366,7 +366,8 @@ int restir_gi_specular_wavefront(const RestirParams* params, const RestirScene* 
 /* The running mean of the composite in FP64 (fs_reference.sc):
  * mean = mean * (1 - w) + color * w with w = 1 / (frames + 1), NaN colours
  * keep the mean. mean: 3 planes of width * height doubles (r, g, b);
- * alpha: one byte per pixel, the composite's alpha of the last frame. */
+ * alpha: one byte per pixel, the composite's alpha of the last frame.
+ * Images of more than 2^32 - 1 pixels return RESTIR_ERROR_TOO_LARGE. */
 int restir_reference_accumulate(const RestirParams* params, const uint16_t* hdr, double* mean,
 	uint8_t* alpha, uint32_t frames, void* stream);
 
@@ -376,22 +377,24 @@ uint64_t restir_error_scratch_bytes(uint32_t width, uint32_t height);
 /* The error of an image against the reference (cs_error.sc), reduced in
  * FP64 in a fixed order: out[0] relative MSE, out[1] mean luminance of the
  * image, out[2] mean luminance of the reference, out[3] pixels compared.
- * scratch: restir_error_scratch_bytes bytes of device memory. */
+ * scratch: restir_error_scratch_bytes bytes of device memory. Images of more
+ * than 2^32 - 1 pixels return RESTIR_ERROR_TOO_LARGE. */
 int restir_error(const RestirParams* params, const uint16_t* display, const double* mean,
 	const uint8_t* alpha, double* out, void* scratch, void* stream);
 
-/* restir_error for callers that cannot allocate device memory: code running
- * inside a frame that is being recorded into a CUDA graph (cudaMalloc is not
- * a stream operation and cannot be captured), hosts such as game engines
- * whose memory manager owns the whole device budget, and real-time loops that
- * must never enter the driver's allocator (it can synchronise the device).
- * No counterpart in the reference. The caller passes only inputs and the
- * 4-double output; the reduction's partial records live in a 64 KB array
+/* restir_error for callers that cannot allocate device memory: hosts such as
+ * game engines whose own memory manager owns the whole device budget and
+ * hands out no more, and real-time loops that must never enter the driver's
+ * allocator (cudaMalloc and cudaFree can synchronise the device and stall the
+ * frame). No counterpart in the reference. The caller passes only inputs and
+ * the 4-double output; the reduction's partial records live in a 64 KB array
  * inside the library, which every device that loads the library keeps until
  * the process exits. Limit: width * height <= 8,388,608 pixels (3840x2160
  * fits); larger images return RESTIR_ERROR_TOO_LARGE. The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress) with
- * that device current, so make it before any stream capture. All calls share
+ * that device current, so make it before any stream capture; the address is
+ * kept until the process exits, so do not call this entry point again after
+ * resetting the device (cudaDeviceReset) in the same process. All calls share
  * the one array: calls whose kernels overlap on the GPU (on two streams, say)
  * race on it and must be ordered by the caller. Nothing in the array needs
  * to start at zero; each call overwrites the records it reads. */

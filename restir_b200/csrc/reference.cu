@@ -181,7 +181,12 @@ extern "C" int restir_reference_accumulate(const RestirParams* params, const uin
 	{
 		return RESTIR_ERROR_INVALID_ARGUMENT;
 	}
-	const uint32_t n = params->width * params->height;
+	const uint64_t pixels = uint64_t(params->width) * params->height;
+	if (pixels > uint64_t(UINT32_MAX))
+	{
+		return RESTIR_ERROR_TOO_LARGE;
+	}
+	const uint32_t n = uint32_t(pixels);
 	uint32_t blocks = (n + 255u) / 256u;
 	blocks = blocks < 148u * 16u ? blocks : 148u * 16u;
 	accumulateKernel<<<blocks, 256, 0, asStream(stream)>>>(hdr, mean, alpha, n, 1.0 / double(frames + 1u));
@@ -202,6 +207,10 @@ extern "C" int restir_error(const RestirParams* params, const uint16_t* display,
 		|| params->width == 0 || params->height == 0 || (reinterpret_cast<uintptr_t>(scratch) & 7u) != 0u)
 	{
 		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	if (uint64_t(params->width) * params->height > uint64_t(UINT32_MAX))
+	{
+		return RESTIR_ERROR_TOO_LARGE;
 	}
 	return launchError(params, display, mean, alpha, out, static_cast<double*>(scratch), asStream(stream));
 }

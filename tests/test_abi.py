@@ -51,3 +51,18 @@ def test_struct_layouts_match_the_binding():
     for name, cls in structs.items():
         assert lib.restir_struct_size(name.encode()) == C.sizeof(cls), name
     assert lib.restir_struct_size(b"NoSuchStruct") == 0
+
+
+def test_fp64_passes_refuse_images_beyond_32_bit_pixel_counts():
+    """restir_reference_accumulate and restir_error count pixels in 32 bits:
+    a 65536 x 65536 image is refused before anything is launched (no device
+    memory is touched, so this runs without a GPU)."""
+    import ctypes as C
+
+    from restir_b200.abi import RestirParams
+    lib = rb.load()
+    p = RestirParams()
+    p.width, p.height = 65536, 65536
+    fake = C.c_void_p(256)
+    assert lib.restir_reference_accumulate(p, fake, fake, fake, 0, None) == rb.ERROR_TOO_LARGE
+    assert lib.restir_error(p, fake, fake, fake, fake, fake, None) == rb.ERROR_TOO_LARGE

@@ -1,10 +1,9 @@
 """The allocation-free error pass, restir_error_noalloc.
 
 Some callers of this library cannot allocate device memory when they run the
-error pass: a frame being recorded into a CUDA graph (an allocation is not a
-stream operation and cannot be captured), an engine whose own memory manager
-owns the whole device budget, a real-time loop that must not enter the
-driver's allocator. For them the library keeps the pass's scratch (the
+error pass: an engine whose own memory manager owns the whole device budget,
+or a real-time loop that must not enter the driver's allocator (cudaMalloc and
+cudaFree can synchronise the device). For them the library keeps the pass's scratch (the
 per-block FP64 partial records) in a fixed 64 KB array of its own, and the
 entry point takes only inputs and the output.
 
