@@ -1,5 +1,6 @@
-"""ORACLE (test infrastructure): ctypes binding of oracle/liboracle.so and of
-the reference's own BVH and light-list builders compiled in oracle/_ref.
+"""ORACLE (test infrastructure): ctypes binding of oracle/liboracle.so, of
+the reference's own BVH and light-list builders compiled in oracle/_ref, and
+of the reference's own shader code compiled there (libref_shaders.so).
 
 The oracle's entry points take the arguments of the CUDA ABI's passes with
 host (numpy) buffers instead of device pointers.
@@ -18,6 +19,7 @@ from restir_b200.abi import (RestirDiReservoirs, RestirDisplayParams, RestirGBuf
 HERE = Path(__file__).resolve().parent
 LIBRARY = HERE / "liboracle.so"
 REFERENCE_LIBRARY = HERE / "_ref" / "libref_bvh.so"
+SHADER_LIBRARY = HERE / "_ref" / "libref_shaders.so"
 
 P = C.c_void_p
 u32 = C.c_uint32
@@ -62,8 +64,25 @@ _SIGNATURES = {
     "oracle_cache_adam": (None, [P, u32, P, P, P, P, C.c_float, C.c_float]),
 }
 
+# The reference's shader passes (oracle/ref_shim/ref_passes.cpp): the
+# arguments of the oracle function of the same name.
+_SHADER_SIGNATURES = {
+    "ref_trace": (C.c_int, [PS, P, P, P, u32, C.c_int]),
+    "ref_grid_keys": (C.c_int, [P, P, u32, P, P, P, u32, P, P, P]),
+    "ref_grid_insert": (C.c_int, [PP, PG, P]),
+    "ref_gi_temporal": _SIGNATURES["oracle_gi_temporal"],
+    "ref_gi_spatial": _SIGNATURES["oracle_gi_spatial"],
+    "ref_di_temporal": _SIGNATURES["oracle_di_temporal"],
+    "ref_di_spatial": _SIGNATURES["oracle_di_spatial"],
+    "ref_svgf_variance": _SIGNATURES["oracle_svgf_variance"],
+    "ref_svgf_atrous": _SIGNATURES["oracle_svgf_atrous"],
+    "ref_composite_specular": _SIGNATURES["oracle_composite_specular"],
+    "ref_gi_specular": _SIGNATURES["oracle_gi_specular"],
+}
+
 _lib = None
 _ref = None
+_shaders = None
 
 
 def load() -> C.CDLL:
@@ -136,3 +155,20 @@ def reference_lights(extra_count: int, extra_intensity: float, extra_seed: int, 
     if count:
         lib.ref_copy_lights(data.ctypes.data)
     return data, count, triangles.value
+
+
+def shaders_available() -> bool:
+    return SHADER_LIBRARY.exists()
+
+
+def load_shaders() -> C.CDLL:
+    """The reference's shader passes compiled as C++ (oracle/ref_shim), built by oracle/Makefile."""
+    global _shaders
+    if _shaders is None:
+        lib = C.CDLL(str(SHADER_LIBRARY))
+        for name, (restype, argtypes) in _SHADER_SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = restype
+            fn.argtypes = argtypes
+        _shaders = lib
+    return _shaders

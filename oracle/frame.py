@@ -5,7 +5,10 @@ CPU baseline.
 FrameRunner owns one frame's buffers and history with the reference's
 ping-pong (renderer.h:218-219, renderer.cpp:706, 1122) and runs the passes in
 the reference's order. backend="oracle" calls oracle/liboracle.so on numpy
-arrays; backend="cuda" calls restir_b200's C ABI on torch tensors on cuda:0.
+arrays; backend="cuda" calls restir_b200's C ABI on torch tensors on cuda:0;
+backend="ref" calls the reference's own shader code compiled as C++
+(oracle/_ref/libref_shaders.so) for the passes it has (REF_PASSES) and the
+oracle for the rest.
 In check mode (run_checked) every CUDA pass is fed the oracle's inputs and
 its outputs are compared with the oracle's bit for bit, pass by pass.
 
@@ -22,6 +25,13 @@ import restir_b200 as rb
 from restir_b200.abi import RestirDiReservoirs, RestirGBuffer, RestirGiHistory, RestirGiReservoirs
 
 from . import binding as ob
+
+# Passes the reference's compiled shader code runs (backend "ref"): the
+# compute and fragment passes of the light transport. The ray-cast stand-ins
+# for the raster passes (G-buffer, shadow atlas), the FP64 reference and the
+# display chain stay with the oracle.
+REF_PASSES = ("grid_insert", "gi_temporal", "gi_spatial", "di_temporal", "di_spatial", "svgf_variance",
+              "svgf_atrous", "composite_specular", "gi_specular")
 
 # name: (dtype, channels, resolution) with resolution "full", "gi", "atlas", "grid", "none"
 LAYOUT = {
@@ -83,6 +93,7 @@ class FrameRunner:
         else:
             self.scene = setup.host_scene()
             self.lib = ob.load()
+            self.shader_lib = ob.load_shaders() if backend == "ref" else None
         self.error_scratch = None
         # The radiance cache (settings.radiance_cache): the cuda backend owns it;
         # the oracle backend takes its values per pass (cache_values) from there.
@@ -110,6 +121,8 @@ class FrameRunner:
     def call(self, name, *args):
         if self.backend == "cuda":
             rb.check(getattr(self.lib, "restir_" + name)(*args, None), name)
+        elif self.backend == "ref" and name in REF_PASSES:
+            rb.check(getattr(self.shader_lib, "ref_" + name)(*args), "ref_" + name)
         else:
             rb.check(getattr(self.lib, "oracle_" + name)(*args), name)
 
@@ -335,6 +348,39 @@ class FrameRunner:
     def host(self, name) -> np.ndarray:
         v = self.buffers[name]
         return v.cpu().numpy() if hasattr(v, "cpu") else v
+
+
+def run_pinned(setup, width: int, height: int, frames: int, settings=None):
+    """Runs `frames` frames with the oracle and with the reference's own
+    shader code, feeding each reference pass the oracle's inputs and
+    comparing its outputs bit for bit. Returns ({pass: mismatching elements},
+    {pass the reference's code ran: output elements it changed})."""
+    oracle_run = FrameRunner(setup, width, height, "oracle", settings)
+    ref_run = FrameRunner(setup, width, height, "ref", settings)
+    report, pinned = {}, {}
+    for frame in range(frames):
+        oracle_run.prepare()
+        ref_run.prepare()
+        for (name, o_fn), (_, r_fn) in zip(oracle_run.passes(), ref_run.passes()):
+            before = {k: v.copy() for k, v in oracle_run.buffers.items()}
+            for k, v in before.items():
+                ref_run.buffers[k][...] = v
+            o_fn()
+            r_fn()
+            base = name.rstrip("0123456789")
+            base = "composite_specular" if base == "composite" else base
+            if base not in REF_PASSES:
+                continue
+            for k in before:
+                want, got = oracle_run.buffers[k], ref_run.buffers[k]
+                changed = int(np.count_nonzero(got.view(np.uint8) != before[k].view(np.uint8)))
+                pinned[base] = pinned.get(base, 0) + changed
+                bad = int(np.count_nonzero(got.view(np.uint8) != want.view(np.uint8)))
+                if bad:
+                    report[f"{frame}:{name}:{k}"] = bad
+        oracle_run.finish()
+        ref_run.finish()
+    return report, pinned
 
 
 def run_checked(setup, width: int, height: int, frames: int, settings=None, on_mismatch=None,

@@ -3,7 +3,7 @@
 Usage: python glsl_to_cpp.py <shader directory> <output directory>
 
 Every *.sh and *.sc file of the reference's shader directory is written to
-the output directory with three mechanical changes and nothing else, so that
+the output directory with the mechanical changes below and nothing else, so that
 it compiles as C++ against oracle/ref_shim/shader_shim.h:
 
   * comments become blanks (newlines kept, so compiler messages keep the
@@ -12,6 +12,9 @@ it compiles as C++ against oracle/ref_shim/shader_shim.h:
     precision, C++ ones double, and a double literal would widen the
     arithmetic around it;
   * `out T name` and `inout T name` parameters become `T& name`;
+  * a global declared `static` (a shader's private, per-invocation global,
+    such as bvh.sh's g_bvhThread) becomes `static thread_local`, since the
+    lanes of a group run as threads;
   * GLSL evaluates a call's arguments left to right, C++ in no set order
     (g++ goes right to left): where one statement passes the results of
     several calls that update the same state through an `inout` parameter
@@ -21,9 +24,10 @@ it compiles as C++ against oracle/ref_shim/shader_shim.h:
     has an `out`/`inout` parameter is refused, so nothing is reordered
     silently.
 
-`#include <bgfx_compute.sh>` / `<bgfx_shader.sh>` are dropped (the shim is
-included first) and `#include "shaderlib.sh"` too (the shim has the three
-helpers the shaders use). The output goes to oracle/_ref/, which is never
+`#include <bgfx_compute.sh>`, `<bgfx_shader.sh>`, `<common.sh>` and
+`"shaderlib.sh"` are dropped (the shim is included first and has the three
+shaderlib helpers the shaders use), and so are the fragment shaders' bgfx
+varying lines (`$input v_texcoord0`: the shim supplies v_texcoord0). The output goes to oracle/_ref/, which is never
 committed: the shader sources stay where they are.
 """
 from __future__ import annotations
@@ -35,8 +39,10 @@ from pathlib import Path
 COMMENT = re.compile(r"//[^\n]*|/\*.*?\*/", re.S)
 FLOAT = re.compile(r"(?<![\w.])((?:\d+\.\d*|\.\d+)(?:[eE][+-]?\d+)?|\d+[eE][+-]?\d+)(?![\w.])")
 QUALIFIED = re.compile(r"\b(?:inout|out)\s+([A-Za-z_]\w*)\s+(_?[A-Za-z]\w*)")
+PRIVATE_GLOBAL = re.compile(r"^static(?=\s+(?!const\b))", re.M)
 IN_QUALIFIED = re.compile(r"([(,]\s*)in\s+([A-Za-z_]\w*\s+_?[A-Za-z]\w*)")
-DROPPED = re.compile(r'^[ \t]*#[ \t]*include[ \t]*(?:<bgfx_(?:compute|shader)\.sh>|"shaderlib\.sh")[^\n]*$', re.M)
+DROPPED = re.compile(r'^[ \t]*(?:#[ \t]*include[ \t]*(?:<bgfx_(?:compute|shader)\.sh>|<common\.sh>|"shaderlib\.sh")'
+                     r'|\$(?:input|output)\b)[^\n]*$', re.M)
 
 
 def blank(match: re.Match) -> str:
@@ -87,6 +93,7 @@ def translate(text: str, writers: set[str]) -> str:
     text = FLOAT.sub(lambda m: m.group(1) + "f", text)
     text = QUALIFIED.sub(lambda m: f"{m.group(1)}& {m.group(2)}", text)
     text = IN_QUALIFIED.sub(lambda m: m.group(1) + m.group(2), text)
+    text = PRIVATE_GLOBAL.sub("static thread_local", text)
     return text
 
 

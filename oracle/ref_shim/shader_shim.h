@@ -518,7 +518,8 @@ void barrier();
 inline void memoryBarrierShared() {}
 inline void GroupMemoryBarrierWithGroupSync() { barrier(); }
 
-// Fragment built-ins.
+// Fragment built-ins and the full-screen pass's varying (the texel centre).
+extern thread_local vec2 v_texcoord0;
 extern thread_local vec4 gl_FragCoord;
 extern thread_local vec4 gl_FragColor;
 extern thread_local vec4 gl_FragData[4];

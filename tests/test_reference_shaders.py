@@ -111,3 +111,46 @@ def test_grid_insert_equals_reference_cs_grid_insert(scene, size):
     assert ref().ref_grid_insert(params, gbuffer_struct(gbuffer), want.ctypes.data) == 0
     np.testing.assert_array_equal(got, want)
     assert np.count_nonzero(want[:T]) > 20
+
+
+FRAME_CASES = {
+    # Cornell box, full-resolution GI, point light and emissive panel.
+    "cornell": dict(scene=(rb.SCENE_CORNELL, 0, 0), size=(64, 64), frames=3, overrides=dict(gi_divisor=1)),
+    # Courtyard with sky, half-resolution GI, 64 extra point lights and the emissive triangles in DI.
+    "courtyard": dict(scene=(rb.SCENE_COURTYARD, 0, 20000), size=(128, 72), frames=3,
+                      overrides=dict(extra_lights=64)),
+    # Every GI ray through the BVH, 4 candidates per pixel.
+    "bvh-rays": dict(scene=(rb.SCENE_CORNELL, 0, 0), size=(48, 48), frames=2,
+                     overrides=dict(gi_divisor=1, ray_mode=rb.RAY_BVH, initial_candidates=4)),
+    # Depth buffer only, screen-space reuse, GI without DI, no denoiser.
+    "screen-space": dict(scene=(rb.SCENE_COURTYARD, 0, 20000), size=(96, 54), frames=3,
+                         overrides=dict(ray_mode=rb.RAY_SCREEN, world_space_reuse=0, direct_lighting=1,
+                                        denoiser=0)),
+}
+
+
+@pytest.mark.parametrize("case", list(FRAME_CASES))
+def test_frame_passes_equal_reference_shaders(case):
+    """Every pass the reference runs as a compute or fragment shader (grid
+    insert, GI temporal with its 4x8 groups and barriers, GI spatial, DI
+    temporal and spatial, SVGF variance and a-trous, composite, specular),
+    over frames that carry history, gives the oracle's outputs bit for bit
+    when both get the same inputs."""
+    from oracle.frame import run_pinned
+    c = FRAME_CASES[case]
+    setup = make_scene(*c["scene"], extra_lights=c["overrides"].get("extra_lights", 0))
+    settings = setup.settings
+    for k, v in c["overrides"].items():
+        setattr(settings, k, v)
+    settings.grid_mode = rb.GRID_DETERMINISTIC
+    if "extra_lights" in c["overrides"]:
+        setup.lights = rb.Lights(setup.bvh, setup.mesh, settings)
+    w, h = c["size"]
+    report, pinned = run_pinned(setup, w, h, c["frames"], settings)
+    assert report == {}, report
+    expected = {"grid_insert", "gi_temporal", "gi_spatial", "composite_specular"}
+    if case != "screen-space":
+        expected |= {"di_temporal", "di_spatial", "svgf_variance", "svgf_atrous", "gi_specular"}
+    assert expected <= set(pinned), pinned
+    # Every pinned pass wrote output, so the equality is not of untouched buffers.
+    assert all(pinned[name] > 0 for name in expected), pinned
