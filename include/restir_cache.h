@@ -205,6 +205,15 @@ int restir_cache_train_frame(const RestirParams* params, const RestirScene* scen
 	const float* shadow_atlas, const RestirCacheConfig* cache_config, void* cache_state, void* workspace,
 	uint64_t workspace_bytes, void* stream);
 
+/* A check of the bounded wait that guards every tensor-core step (no
+ * reference counterpart): one block waits, exactly as the cache's kernels
+ * wait for their MMAs, on an mbarrier that no one arrives at, for at most
+ * `polls` polls (1 to 4,194,304), and no MMA is issued. The wait gives up,
+ * raises status bit 3 (value 8, read and cleared by restir_status) and the
+ * kernel returns; *result (device memory) is 0 then. Lets a test show that
+ * a failed tensor-core step ends with an error status instead of a hang. */
+int restir_cache_wait_check(uint32_t polls, uint32_t* result, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -392,6 +392,9 @@ def run_checked(setup, width: int, height: int, frames: int, settings=None, on_m
     cuda_run = FrameRunner(setup, width, height, "cuda", settings, gi_wavefront=gi_wavefront)
     assert oracle_run.radiance_cache == cuda_run.radiance_cache
     report = {}
+    # Buffers whose device copy may differ from the oracle's: all at first,
+    # then those the last pass changed (the CUDA pass wrote its own values).
+    stale = set(oracle_run.buffers)
     for frame in range(frames):
         if reference_frames and frame == frames - reference_frames:
             oracle_run.set_reference_accumulation(True)
@@ -401,8 +404,8 @@ def run_checked(setup, width: int, height: int, frames: int, settings=None, on_m
         for (name, o_fn), (_, c_fn) in zip(oracle_run.passes(), cuda_run.passes()):
             before = {k: v.copy() for k, v in oracle_run.buffers.items()}
             # The CUDA pass gets exactly the oracle's inputs.
-            for k, v in before.items():
-                cuda_run.buffers[k].copy_(torch.from_numpy(v))
+            for k in stale:
+                cuda_run.buffers[k].copy_(torch.from_numpy(before[k]))
             if cuda_run.radiance_cache and name in ("gi_temporal", "gi_spatial", "cache_train"):
                 # The cache lives on the GPU: the CUDA pass runs first and the
                 # oracle takes the cache values it read.
@@ -416,6 +419,7 @@ def run_checked(setup, width: int, height: int, frames: int, settings=None, on_m
                 c_fn()
                 torch.cuda.synchronize()
             changed = [k for k in before if not np.array_equal(before[k], oracle_run.buffers[k])]
+            stale = set(changed) | ({k for k in before if k.startswith("grid")} if name.startswith("grid") else set())
             for k in changed + [k for k in before if k not in changed and name.startswith("grid")]:
                 got = cuda_run.host(k)
                 want = oracle_run.buffers[k]

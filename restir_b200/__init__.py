@@ -167,6 +167,7 @@ _SIGNATURES = {
     "restir_gi_spatial_cached": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirScene), C.POINTER(RestirGBuffer),
                                            C.POINTER(RestirGiReservoirs), P, C.POINTER(RestirGiHistory), P, P, P, P,
                                            C.POINTER(abi.RestirCacheConfig), P, P, C.c_uint64, P]),
+    "restir_cache_wait_check": (C.c_int, [u32, P, P]),
     "restir_cache_train_frame": (C.c_int, [C.POINTER(RestirParams), C.POINTER(RestirScene), C.POINTER(RestirGBuffer),
                                            P, C.POINTER(abi.RestirCacheConfig), P, P, C.c_uint64, P]),
 }

@@ -228,14 +228,12 @@ struct TensorContext
 	bool ok;
 };
 
-// Commit by the issuing thread, then every thread waits for the MMAs.
-__device__ __forceinline__ void completeMmas(TensorContext& t)
+// Every thread waits for the barrier's current phase, at most `polls` polls;
+// a wait that gives up raises status bit 3 and marks the context failed (the
+// kernel then skips its remaining tensor-core steps and frees its TMEM).
+__device__ __forceinline__ void awaitBarrier(TensorContext& t, uint32_t polls)
 {
-	if (threadIdx.x == 0)
-	{
-		umma::commit(t.barrier);
-	}
-	bool done = umma::barrierWait(t.barrier, t.phase, kWaitPolls);
+	bool done = umma::barrierWait(t.barrier, t.phase, polls);
 	t.phase ^= 1u;
 	done = __syncthreads_and(done) != 0;
 	if (!done)
@@ -247,6 +245,38 @@ __device__ __forceinline__ void completeMmas(TensorContext& t)
 		t.ok = false;
 	}
 	umma::fenceAfterSync();
+}
+
+// Commit by the issuing thread, then every thread waits for the MMAs.
+__device__ __forceinline__ void completeMmas(TensorContext& t)
+{
+	if (threadIdx.x == 0)
+	{
+		umma::commit(t.barrier);
+	}
+	awaitBarrier(t, kWaitPolls);
+}
+
+// The failure path of the bounded wait, with no MMA: an mbarrier that no one
+// arrives at, waited on as completeMmas waits (restir_cache_wait_check).
+__global__ void __launch_bounds__(128) waitCheckKernel(uint32_t polls, uint32_t* result)
+{
+	__shared__ __align__(8) uint64_t barrier;
+	TensorContext t;
+	t.barrier = umma::smemAddress(&barrier);
+	t.phase = 0;
+	t.ok = true;
+	t.tmem = 0;
+	if (threadIdx.x == 0)
+	{
+		umma::barrierInit(t.barrier, 1);
+	}
+	__syncthreads();
+	awaitBarrier(t, polls);
+	if (threadIdx.x == 0)
+	{
+		*result = t.ok ? 1u : 0u;
+	}
 }
 
 // The descriptors address the tiles from the start of dynamic shared memory,
@@ -1086,4 +1116,18 @@ extern "C" int restir_cache_train(const RestirCacheConfig* cfg, void* state, con
 {
 	const int status = restir_cache_gradients(cfg, state, queries, targets, n, stream);
 	return status != RESTIR_OK ? status : restir_cache_adam(cfg, state, stream);
+}
+
+// A check of the tensor-core steps' bounded wait, no counterpart in the
+// reference: one block waits, as completeMmas does, on an mbarrier that no
+// one arrives at, for at most `polls` polls; the wait gives up, raises status
+// bit 3 and the kernel returns. result (device): 0 when the wait gave up.
+extern "C" int restir_cache_wait_check(uint32_t polls, uint32_t* result, void* stream)
+{
+	if (result == nullptr || polls == 0u || polls > kWaitPolls)
+	{
+		return RESTIR_ERROR_INVALID_ARGUMENT;
+	}
+	waitCheckKernel<<<1, 128, 0, asStream(stream)>>>(polls, result);
+	return launchStatus();
 }

@@ -222,3 +222,43 @@ def test_reference_accumulation_and_error_fp64():
     got = cuda_run.error()
     np.testing.assert_allclose(got, want, rtol=1e-12, atol=0)
     assert want[3] > 0
+
+
+@pytest.mark.gpu
+def test_bench_configuration_frames_bit_exact():
+    """The frame the benchmark times (1920x1080, the seeded 1M-triangle city,
+    64 extra point lights beside its emissive panels, the reference's default
+    settings: half-resolution GI with 2 candidates, 2 temporal and 4 spatial
+    taps, ReSTIR DI, specular GI, SVGF with 5 a-trous levels, TAA and AgX),
+    through the renderer's wavefront passes, three frames with history, every
+    pass bit for bit against the oracle given the oracle's inputs. The grid
+    runs in its deterministic mode (the atomic mode keeps the first 32
+    arrivals per cell, which depends on scheduling)."""
+    setup = make_scene(rb.SCENE_CITY, 0, 1_000_000, extra_lights=64)
+    settings = setup.settings
+    settings.grid_mode = rb.GRID_DETERMINISTIC
+    assert (settings.gi_divisor, settings.initial_candidates, settings.atrous_iterations) == (2, 2, 5)
+    rb.status_flags()
+    report, oracle_run, cuda_run = run_checked(setup, 1920, 1080, 3, settings, gi_wavefront=True)
+    assert report == {}, report
+    assert setup.lights.count == 320 and setup.bvh.desc.triangle_count > 990_000
+    gi = oracle_run.host("gi.color1" if oracle_run.history_read == 1 else "gi.color0")
+    assert np.count_nonzero(gi) > 0.2 * gi.size
+    assert rb.status_flags() & (2 | 4) == 0  # no probe-cap or queue overflow
+
+
+@pytest.mark.gpu
+def test_small_configuration_sixteen_frames_bit_exact():
+    """The small configuration as stated: the procedural open-front Cornell box
+    at 256x256, full-resolution GI (d = 1) with 1 candidate per pixel, a
+    2^16-slot hash grid, GI temporal and spatial reuse, 16 static frames,
+    seed 0; every pass of every frame bit for bit against the oracle."""
+    setup = make_scene(rb.SCENE_CORNELL, 0, 0)
+    settings = setup.settings
+    settings.gi_divisor = 1
+    settings.initial_candidates = 1
+    settings.grid_mode = rb.GRID_DETERMINISTIC
+    assert settings.grid_table_size == 1 << 16 and settings.temporal_taps > 0 and settings.spatial_taps > 0
+    report, oracle_run, _ = run_checked(setup, 256, 256, 16, settings, gi_wavefront=True)
+    assert report == {}, report
+    assert oracle_run.state.frame_number == 16
