@@ -52,6 +52,8 @@ ERROR_FRAMES = 240         # frames the relMSE is averaged over (it swings by +-
 DOMINANT_TRAFFIC = {"gi_temporal": 134.9e6}
 SIDE_STREAM_PASSES = ("shadow", "specular")
 CACHE_TRAIN_FRAMES = 60    # online training before the radiance-cache form is timed
+WORKLOAD = ("1920x1080 frame, seeded 1M-triangle city scene, GI 1/2 res + DI + specular GI + SVGF x5 + TAA + AgX "
+            "tone mapping")
 
 # Algorithmic (compulsory) bytes per pixel of each pass's image reads and
 # writes, besides its BVH traversal (32 B per node fetch, 48 B per triangle
@@ -148,59 +150,69 @@ def scene_and_settings(rb):
     return mesh, settings
 
 
-def cpu_baseline(steps: int = 1, scale: int = 4) -> dict:
-    """The oracle (CPU restatement, all host threads) on a bounded sample of the
-    same workload: one frame at 1/scale of the resolution in each axis and a
-    shadow atlas of 1/scale the face size, each pass's time multiplied by
-    scale^2 (its pixels or texels)."""
+def cpu_frames(steps: int, warmup: int) -> dict:
+    """The reference's per-frame path on the host cores, full frames of the
+    same workload: the seeded 1M-triangle city at 1920x1080 with the
+    reference's default settings, its BVH and light list from the reference's
+    own src/bvh.cpp and src/lights.cpp (oracle/_ref/libref_bvh.so), the frame
+    uniforms from the oracle's restatement of renderer.cpp, and every compute
+    and fragment pass the reference runs as a shader (grid insert, GI
+    temporal and spatial, DI temporal and spatial, SVGF, composite, specular)
+    from the reference's own shader code compiled as C++
+    (oracle/_ref/libref_shaders.so); the G-buffer and shadow-atlas ray casts
+    (the reference rasterizes them) and TAA and tone mapping come from the
+    oracle. All host threads. Nothing of this repository's library is loaded.
+    `warmup` untimed frames (history), then `steps` timed frames."""
     import oracle.binding as ob
-    import restir_b200 as rb
     from oracle.frame import FrameRunner
-    from tests.helpers import make_scene
+    from oracle.workload import OracleSetup
+    import restir_b200 as rb
 
-    setup = make_scene(rb.SCENE_CITY, 0, TRIANGLES, extra_lights=EXTRA_LIGHTS)
-    settings = setup.settings
-    settings.shadow_face_size = 512 // scale
-    runner = FrameRunner(setup, WIDTH // scale, HEIGHT // scale, "oracle", settings)
-    runner.render()  # history for the temporal passes
-    totals = []
+    threads = os.cpu_count() or 1
+    ob.load().oracle_set_threads(threads)
+    ob.load_shaders().ref_set_threads(threads)
+    t = time.perf_counter()
+    setup = OracleSetup(rb.SCENE_CITY, 0, TRIANGLES, extra_lights=EXTRA_LIGHTS)
+    setup_ms = (time.perf_counter() - t) * 1e3
+    runner = FrameRunner(setup, WIDTH, HEIGHT, "ref", setup.settings)
+    for _ in range(warmup):
+        runner.render()
+    times, pass_ms = [], {}
     for _ in range(steps):
         runner.prepare()
-        elapsed = 0.0
-        for _, fn in runner.passes():
+        start = time.perf_counter()
+        for name, fn in runner.passes():
             t = time.perf_counter()
             fn()
-            elapsed += time.perf_counter() - t
+            pass_ms[name] = pass_ms.get(name, 0.0) + (time.perf_counter() - t) * 1e3 / steps
         runner.finish()
-        totals.append(elapsed * scale * scale * 1e3)
-    return {"value": float(np.median(totals)), "unit": "ms/frame", "cores": ob.load().oracle_get_threads(),
-            "kind": "port",
-            "sample": f"{steps} frame(s) at {WIDTH // scale}x{HEIGHT // scale} with a {3 * (512 // scale)}x"
-                      f"{2 * (512 // scale)} shadow atlas on the same 1M-triangle scene, each pass's time x{scale * scale}"}
+        times.append((time.perf_counter() - start) * 1e3)
+    return {"value": float(np.mean(times)), "unit": "ms/frame", "cores": threads, "kind": "reference",
+            "sample": f"{steps} full {WIDTH}x{HEIGHT} frame(s) of the {setup.mesh.triangle_count}-triangle city after "
+                      f"{warmup} history frame(s): the reference's shader code (compiled as C++) for its compute and "
+                      f"fragment passes, its bvh.cpp/lights.cpp for the scene; ray-cast G-buffer and shadow atlas, TAA "
+                      f"and tone mapping from the oracle",
+            "frame_ms": [float(v) for v in times], "pass_ms": {k: float(v) for k, v in pass_ms.items()},
+            "scene_setup_ms": setup_ms, "scene_triangles": int(setup.mesh.triangle_count)}
 
 
 def reference_arm(args, rank: int, world: int) -> None:
-    """--impl reference: the reference's per-frame path on the host cores. The
-    reference runs it in bgfx shaders (no CPU implementation, and no graphics
-    stack here), so this is the oracle's C++ restatement of its shaders."""
+    """--impl reference: the reference's per-frame path on the host cores
+    (cpu_frames), one full frame per step. The reference runs the path as
+    bgfx shaders; with no graphics stack here its own shader code runs on the
+    CPU, compiled as C++. Under torchrun only rank 0 works."""
     if rank != 0:
         return
-    times = []
-    baseline = None
-    for step in range(args.warmup + args.steps):
-        t = time.perf_counter()
-        baseline = cpu_baseline(steps=1, scale=4)
-        if step >= args.warmup:
-            times.append(baseline["value"])
-    value = float(np.mean(times))
+    result = cpu_frames(args.steps, args.warmup)
+    value = result["value"]
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "ms/frame", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"1920x1080 frame, seeded 1M-triangle city scene, GI 1/2 res + DI + specular GI + SVGF x5 + TAA + AgX tone mapping",
-                   "scene_triangles": TRIANGLES, "width": WIDTH, "height": HEIGHT},
-        "cpu_baseline": {"value": value, "unit": "ms/frame", "cores": baseline["cores"], "kind": "port",
-                         "sample": baseline["sample"]},
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+        "config": {"workload": WORKLOAD, "scene_triangles": result["scene_triangles"], "width": WIDTH,
+                   "height": HEIGHT},
+        "cpu_baseline": {k: result[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "pass_ms": result["pass_ms"],
         "e2e": {"value": value, "unit": "ms/frame", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -604,13 +616,16 @@ def own_arm(args, rank: int, world: int) -> None:
                 + ((1 + plan.exposure) if plan.display else 0)
                 + ((3 if settings.wavefront else 1) if plan.specular else 0))
 
-    baseline = cpu_baseline(steps=1, scale=2) if not args.no_cpu_baseline else None
+    if args.no_cpu_baseline:
+        baseline = None
+    else:
+        frames = cpu_frames(steps=1, warmup=1)
+        baseline = {k: frames[k] for k in ("value", "unit", "cores", "kind", "sample", "pass_ms")}
     line = {
         "metric": METRIC, "value": ms_per_frame, "unit": "ms/frame", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_frame, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
-        "config": {"workload": "1920x1080 frame, seeded 1M-triangle city scene, GI 1/2 res + DI + specular GI + SVGF x5 + TAA + AgX tone mapping",
-                   "scene_triangles": mesh.triangle_count, "width": WIDTH, "height": HEIGHT,
+        "config": {"workload": WORKLOAD, "scene_triangles": mesh.triangle_count, "width": WIDTH, "height": HEIGHT,
                    "gi_resolution": [params.gi_width, params.gi_height], "di_lights": params.di_light_count,
                    "grid_table_size": params.grid_table_size, "graph": bool(args.graph),
                    "l2": "inputs larger than L2 (BVH 126 MB + frame targets), no flush",

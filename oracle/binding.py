@@ -78,6 +78,8 @@ _SHADER_SIGNATURES = {
     "ref_svgf_atrous": _SIGNATURES["oracle_svgf_atrous"],
     "ref_composite_specular": _SIGNATURES["oracle_composite_specular"],
     "ref_gi_specular": _SIGNATURES["oracle_gi_specular"],
+    "ref_set_threads": (None, [C.c_int]),
+    "ref_get_threads": (C.c_int, []),
 }
 
 _lib = None

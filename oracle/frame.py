@@ -12,8 +12,10 @@ oracle for the rest.
 In check mode (run_checked) every CUDA pass is fed the oracle's inputs and
 its outputs are compared with the oracle's bit for bit, pass by pass.
 
-The frame uniforms come from the library's own host code
-(restir_frame_params), which is host logic, not a pass.
+The frame uniforms come from the setup's host side: the library's own host
+code (restir_frame_params) for tests.helpers.SceneSetup, the oracle's
+restatement (oracle_frame_params) for oracle.workload.OracleSetup, which
+needs nothing of the product's library.
 """
 from __future__ import annotations
 
@@ -56,6 +58,22 @@ LAYOUT = {
 }
 
 
+class ProductHost:
+    """The host side of a frame through the product's library (restir_frame.h)."""
+
+    def frame_params(self, settings, mesh, light_count, bvh, frame_input, state):
+        return rb.frame_params(settings, mesh, light_count, bvh, frame_input, state)
+
+    def advance(self, params, plan, frame_input, state):
+        rb.advance(params, plan, frame_input, state)
+
+    def display_params(self, *args):
+        from restir_b200.abi import RestirDisplayParams
+        out = RestirDisplayParams()
+        rb.check(rb.load().restir_display_params(*args, C.byref(out)), "display_params")
+        return out
+
+
 class FrameRunner:
     def __init__(self, setup, width: int, height: int, backend: str = "oracle", settings=None,
                  gi_wavefront: bool = False):
@@ -76,8 +94,10 @@ class FrameRunner:
         self.display_taa = False
         self.params = None
         self.plan = None
+        self.host_side = getattr(setup, "host_side", None) or ProductHost()
         self.frame_input = rb.frame_input(setup.mesh, width, height)
-        p, _ = rb.frame_params(self.settings, setup.mesh, setup.lights.count, setup.bvh, self.frame_input, self.state)
+        p, _ = self.host_side.frame_params(self.settings, setup.mesh, setup.lights.count, setup.bvh, self.frame_input,
+                                      self.state)
         self.shape = {"full": width * height, "gi": p.gi_width * p.gi_height,
                       "atlas": 6 * p.shadow_face_size * p.shadow_face_size,
                       "grid": p.grid_table_size * (2 + p.grid_cell_capacity), "one": 1}
@@ -127,8 +147,8 @@ class FrameRunner:
             rb.check(getattr(self.lib, "oracle_" + name)(*args), name)
 
     def prepare(self):
-        self.params, self.plan = rb.frame_params(self.settings, self.setup.mesh, self.setup.lights.count,
-                                                 self.setup.bvh, self.frame_input, self.state)
+        self.params, self.plan = self.host_side.frame_params(self.settings, self.setup.mesh, self.setup.lights.count,
+                                                        self.setup.bvh, self.frame_input, self.state)
         return self.params, self.plan
 
     # --- the frame ------------------------------------------------------------------------------------
@@ -233,18 +253,14 @@ class FrameRunner:
         return out
 
     def display_params(self):
-        """The display passes' uniforms from the library's host code (restir_display_params)."""
-        from restir_b200.abi import RestirDisplayParams
+        """The display passes' uniforms (restir_display_params or its restatement)."""
         P, plan, s = self.params, self.plan, self.settings
-        D = RestirDisplayParams()
         inv = (C.c_float * 16)(*P.inv_view_proj)
         previous = (C.c_float * 16)(*self.state.previous_unjittered_view_proj)
-        rb.check(rb.load().restir_display_params(C.cast(inv, C.c_void_p), C.cast(previous, C.c_void_p), P.width, P.height,
-                                                 plan.taa, self.state.taa_valid, plan.exposure,
-                                                 self.state.exposure_valid, s.adaptation_speed,
-                                                 self.frame_input.delta_time, s.exposure_ev, s.tonemapper, 0, 0,
-                                                 C.byref(D)), "display_params")
-        return D
+        return self.host_side.display_params(C.cast(inv, C.c_void_p), C.cast(previous, C.c_void_p), P.width, P.height,
+                                        plan.taa, self.state.taa_valid, plan.exposure, self.state.exposure_valid,
+                                        s.adaptation_speed, self.frame_input.delta_time, s.exposure_ev, s.tonemapper,
+                                        0, 0)
 
     def gi_temporal_wavefront(self, P, gb, history, grid, surface, current):
         import torch
@@ -294,7 +310,7 @@ class FrameRunner:
         return self.gi_workspace[offset:offset + 8 * rows].cpu().numpy().view(np.uint16).copy()
 
     def finish(self):
-        rb.advance(self.params, self.plan, self.frame_input, self.state)
+        self.host_side.advance(self.params, self.plan, self.frame_input, self.state)
         self.history_read = 1 - self.history_read
         self.display_taa = bool(self.plan.display and self.plan.taa)
         if self.plan.specular:

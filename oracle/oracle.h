@@ -56,6 +56,33 @@ void oracle_grid_keys(const float* camera, const float* constants, uint32_t tabl
 /* The host evaluation of restir_numeric_eval's functions (same fn codes). */
 void oracle_numeric_eval(int fn, const float* input, float* output, uint32_t n);
 
+/* The host side of a frame (oracle_frame.cpp): the renderer's defaults, the
+ * uniforms of a frame and the state carried on (renderer.cpp:435-731,
+ * 1119-1124), the display passes' uniforms, and the seeded procedural
+ * workload scenes. Same arguments as the product's restir_settings_default,
+ * restir_frame_params, restir_frame_advance, restir_display_params and
+ * restir_mesh_procedural / _describe / _destroy. */
+struct RestirSettings;
+struct RestirMeshDesc;
+struct RestirBvhDesc;
+struct RestirFrameInput;
+struct RestirFrameState;
+struct RestirFramePlan;
+struct RestirDisplayParams;
+void oracle_settings_default(struct RestirSettings* settings);
+int oracle_frame_params(const struct RestirSettings* settings, const struct RestirMeshDesc* scene, uint32_t light_count,
+	const struct RestirBvhDesc* bvh, const struct RestirFrameInput* input, const struct RestirFrameState* state,
+	RestirParams* params, struct RestirFramePlan* plan);
+void oracle_frame_advance(const RestirParams* params, const struct RestirFramePlan* plan,
+	const struct RestirFrameInput* input, struct RestirFrameState* state);
+int oracle_display_params(const float* inv_view_proj, const float* previous_unjittered_view_proj, uint32_t width,
+	uint32_t height, int taa, int taa_history_valid, int auto_exposure, int exposure_valid, float adaptation_speed,
+	float delta_time, float exposure_ev, int tonemapper, int pass_through, int reference_view,
+	struct RestirDisplayParams* out);
+void* oracle_mesh_procedural(int kind, uint32_t seed, uint32_t target_triangles);
+int oracle_mesh_describe(void* mesh, struct RestirMeshDesc* out);
+void oracle_mesh_destroy(void* mesh);
+
 /* Threads the oracle uses; 0: all hardware threads. */
 void oracle_set_threads(int threads);
 int oracle_get_threads(void);

@@ -7,14 +7,17 @@ the output directory with the mechanical changes below and nothing else, so that
 it compiles as C++ against oracle/ref_shim/shader_shim.h:
 
   * comments become blanks (newlines kept, so compiler messages keep the
-    shader's own line numbers);
+    shader's own line numbers, give or take the line a private global's
+    macro adds below);
   * floating-point literals get an `f` suffix: GLSL literals are single
     precision, C++ ones double, and a double literal would widen the
     arithmetic around it;
   * `out T name` and `inout T name` parameters become `T& name`;
   * a global declared `static` (a shader's private, per-invocation global,
-    such as bvh.sh's g_bvhThread) becomes `static thread_local`, since the
-    lanes of a group run as threads;
+    such as bvh.sh's g_bvhThread) becomes one slot per lane of the running
+    worker (`static thread_local T name_lanes[kMaxLanes]` and a macro that
+    indexes it by the running lane), since a group's lanes are coroutines of
+    one worker thread;
   * GLSL evaluates a call's arguments left to right, C++ in no set order
     (g++ goes right to left): where one statement passes the results of
     several calls that update the same state through an `inout` parameter
@@ -39,7 +42,7 @@ from pathlib import Path
 COMMENT = re.compile(r"//[^\n]*|/\*.*?\*/", re.S)
 FLOAT = re.compile(r"(?<![\w.])((?:\d+\.\d*|\.\d+)(?:[eE][+-]?\d+)?|\d+[eE][+-]?\d+)(?![\w.])")
 QUALIFIED = re.compile(r"\b(?:inout|out)\s+([A-Za-z_]\w*)\s+(_?[A-Za-z]\w*)")
-PRIVATE_GLOBAL = re.compile(r"^static(?=\s+(?!const\b))", re.M)
+PRIVATE_GLOBAL = re.compile(r"^static\s+(?!const\b)([A-Za-z_]\w*)\s+([A-Za-z_]\w*)\s*;", re.M)
 IN_QUALIFIED = re.compile(r"([(,]\s*)in\s+([A-Za-z_]\w*\s+_?[A-Za-z]\w*)")
 DROPPED = re.compile(r'^[ \t]*(?:#[ \t]*include[ \t]*(?:<bgfx_(?:compute|shader)\.sh>|<common\.sh>|"shaderlib\.sh")'
                      r'|\$(?:input|output)\b)[^\n]*$', re.M)
@@ -93,7 +96,8 @@ def translate(text: str, writers: set[str]) -> str:
     text = FLOAT.sub(lambda m: m.group(1) + "f", text)
     text = QUALIFIED.sub(lambda m: f"{m.group(1)}& {m.group(2)}", text)
     text = IN_QUALIFIED.sub(lambda m: m.group(1) + m.group(2), text)
-    text = PRIVATE_GLOBAL.sub("static thread_local", text)
+    text = PRIVATE_GLOBAL.sub(lambda m: f"static thread_local {m.group(1)} {m.group(2)}_lanes[refsh::kMaxLanes]; "
+                              f"\n#define {m.group(2)} {m.group(2)}_lanes[refsh::t_lane]", text)
     return text
 
 

@@ -22,7 +22,9 @@
  *    SHARED, NUM_THREADS) as globals the C interface binds, with point
  *    sampling at floor(uv * size) clamped to the image (the sampling rule of
  *    the C ABI), and the compute built-ins (gl_GlobalInvocationID, ...) as
- *    thread-local values the dispatcher sets;
+ *    per-lane values the dispatcher sets (a group's lanes are coroutines that
+ *    switch at barriers, groups run on all host threads, and SHARED memory is
+ *    one copy per worker thread);
  *  - bgfx shaderlib's clip-space helpers with NDC depth in [0, 1]
  *    (toClipSpaceDepth(d) = d, toClipSpaceY(y) = y when the texture origin is
  *    bottom-left, else -y, clipToWorld divides by w).
@@ -509,11 +511,24 @@ inline uint atomicAdd(uint& _memory, uint _value)
 	return original;
 }
 
-// Compute built-ins, set per invocation by the dispatcher.
-extern thread_local uvec3 gl_GlobalInvocationID;
-extern thread_local uvec3 gl_LocalInvocationID;
-extern thread_local uvec3 gl_WorkGroupID;
-extern thread_local uint gl_LocalInvocationIndex;
+// Compute built-ins, set per invocation by the dispatcher. The lanes of a
+// compute group run as coroutines inside one worker thread (they switch at
+// the shader's barriers), so everything private to an invocation lives in a
+// per-lane slot of the worker's storage, indexed by the running lane.
+constexpr int kMaxLanes = 64;
+struct LaneBuiltins
+{
+	uvec3 globalId;
+	uvec3 localId;
+	uvec3 groupId;
+	uint localIndex = 0u;
+};
+extern thread_local int t_lane;
+extern thread_local LaneBuiltins t_builtins[kMaxLanes];
+#define gl_GlobalInvocationID (refsh::t_builtins[refsh::t_lane].globalId)
+#define gl_LocalInvocationID (refsh::t_builtins[refsh::t_lane].localId)
+#define gl_WorkGroupID (refsh::t_builtins[refsh::t_lane].groupId)
+#define gl_LocalInvocationIndex (refsh::t_builtins[refsh::t_lane].localIndex)
 void barrier();
 inline void memoryBarrierShared() {}
 inline void GroupMemoryBarrierWithGroupSync() { barrier(); }
@@ -546,7 +561,8 @@ inline vec3 clipToWorld(const mat4& _inverse, const vec3& _clip)
 #define BUFFER_RW(_name, _type, _stage) refsh::Buffer<_type> _name
 #define BUFFER_WO(_name, _type, _stage) refsh::Buffer<_type> _name
 #define uniform
-#define SHARED
+// Group-shared memory: one copy per worker thread, which runs one group at a time.
+#define SHARED thread_local
 #define NUM_THREADS(_x, _y, _z)
 #define BGFX_SHADER_LANGUAGE_GLSL 0
 #define BGFX_SHADER_LANGUAGE_HLSL 0
