@@ -46,9 +46,8 @@ TRIANGLES = 1_000_000
 EXTRA_LIGHTS = 64
 REFERENCE_FRAMES = 64
 ERROR_FRAMES = 240         # frames the relMSE is averaged over (it swings by +-0.07 between 30-frame windows)
-# DRAM bytes (read + write) per frame of a pass's kernels, from the committed ncu capture of this
-# workload (profiles/gi_temporal_wavefront_1080p_city1M.md): candidates 15.9 MB, queue tracer
-# 30.7 MB, shading 88.2 MB.
+# DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per frame of the GI temporal pass's
+# three kernels on this workload, one launch each, captured from the current build.
 DOMINANT_TRAFFIC = {"gi_temporal": 134.9e6}
 SIDE_STREAM_PASSES = ("shadow", "specular")
 CACHE_TRAIN_FRAMES = 60    # online training before the radiance-cache form is timed
@@ -80,6 +79,31 @@ PASS_PIXEL_BYTES = {
     # last frame's HDR at the hit 8
     "specular": ("gi", 68),
 }
+
+
+def gather_probe(renderer, repeats: int = 5) -> float:
+    """GB/s of random 32-byte row gathers from the scene's BVH nodes
+    (restir_gather_probe; the node rows fit the L2, where the traversal
+    kernels find them), on the renderer's stream."""
+    import torch
+    import restir_b200 as rb
+    lib = rb.load()
+    pointer, nbytes = renderer.buffer("bvh")
+    params, _, _ = renderer.last_frame()
+    rows = min(int(nbytes // 32), 61_000_000 // 32)  # the node part of the buffer, at most 61 MB
+    blocks, gathers = 148 * 8, 256
+    out = torch.empty(blocks * 256, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.ExternalStream(renderer.stream)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for r in range(repeats + 2):
+        if r == 2:
+            start.record(stream)
+        rb.check(lib.restir_gather_probe(pointer, rows, blocks, gathers, r, out.data_ptr(), renderer.stream),
+                 "gather probe")
+    stop.record(stream)
+    torch.cuda.synchronize()
+    fetched = blocks * 256 * gathers * 32 * repeats
+    return fetched / (start.elapsed_time(stop) * 1e-3) / 1e9
 
 
 def load_peaks() -> tuple[float, str]:
@@ -588,25 +612,36 @@ def own_arm(args, rank: int, world: int) -> None:
         return
 
     ms_per_frame = elapsed_ms / args.steps
-    rays = int(counts[:, 0:4].sum())
+    # BVH rays: primary and shadow-map ray casts, GI closest-hit rays, visibility rays (depth-buffer
+    # marches are reported beside them, not counted as rays).
+    rays = int(counts[:, 0:3].sum())
     passes = rb.PASS_NAMES
     mean_pass = pass_ms.mean(axis=0) if len(pass_ms) else np.zeros(len(passes))
     sizes = {"full": WIDTH * HEIGHT, "gi": params.gi_width * params.gi_height,
              "atlas": 6 * params.shadow_face_size ** 2, "none": 0}
-    pass_bytes = {}
+    _, bvh_bytes = renderer.buffer("bvh")
+    image_bytes, fetched_bytes, pass_bytes = {}, {}, {}
     for i, name in enumerate(passes):
         res, per_pixel = PASS_PIXEL_BYTES[name]
         ran = mean_pass[i] > 0
-        pixel_bytes = sizes[res] * per_pixel + (8 * params.grid_table_size if name == "grid" else 0)
-        pass_bytes[name] = (pixel_bytes + 32 * int(counts[i, 4]) + 48 * int(counts[i, 5])) if ran else 0
+        image_bytes[name] = (sizes[res] * per_pixel + (8 * params.grid_table_size if name == "grid" else 0)) if ran else 0
+        fetched_bytes[name] = (32 * int(counts[i, 4]) + 48 * int(counts[i, 5])) if ran else 0
+        pass_bytes[name] = image_bytes[name] + fetched_bytes[name]
     mean_pass = [float(v) for v in mean_pass]
     # The dominant pass of the main chain: the shadow atlas and the specular pass
     # run on a second, lower-priority stream, so their event intervals include
     # the time they wait behind the chain for free SMs.
     chain = [i for i, name in enumerate(passes) if name not in SIDE_STREAM_PASSES]
     dominant = max(chain, key=lambda i: mean_pass[i])
+    name = passes[dominant]
+    seconds = mean_pass[dominant] * 1e-3
     peak, peak_kind = load_peaks()
-    achieved = float(pass_bytes[passes[dominant]] / (mean_pass[dominant] * 1e-3) / 1e9) if mean_pass[dominant] > 0 else 0.0
+    # Compulsory HBM bytes of the pass: its image reads and writes, and each BVH row it touches
+    # at most once (no more than the whole BVH).
+    footprint = image_bytes[name] + min(fetched_bytes[name], bvh_bytes)
+    achieved = float(footprint / seconds / 1e9) if seconds > 0 else 0.0
+    l2_gather_gbs = gather_probe(renderer)
+    fetched_gbs = float(fetched_bytes[name] / seconds / 1e9) if seconds > 0 else 0.0
     share = {name: (mean_pass[i] / ms_per_frame if ms_per_frame > 0 else 0.0) for i, name in enumerate(passes)}
     # shadow, G-buffer, DI x2, grid x2, GI temporal (3 kernels as a wavefront), GI spatial, denoiser, composite,
     # display (auto exposure when on, then TAA + tone mapping), specular (3 kernels as a wavefront)
@@ -632,7 +667,9 @@ def own_arm(args, rank: int, world: int) -> None:
                    "parallelism": f"replicas x{world}"},
         "mrays_per_s": float(rays / (ms_per_frame * 1e-3) / 1e6),
         "rays_per_frame": {"primary_and_shadow_map": int(counts[:, 0].sum()), "gi_closest": int(counts[:, 1].sum()),
-                           "visibility_any_hit": int(counts[:, 2].sum()), "depth_buffer_marches": int(counts[:, 3].sum())},
+                           "visibility_any_hit": int(counts[:, 2].sum())},
+        "depth_buffer_marches_per_frame": int(counts[:, 3].sum()),
+        "truncated_rays_per_frame": int(counts[:, 7].sum()),
         "rel_mse_vs_fp64_reference": plain_error["mean"], "rel_mse_median": plain_error["median"],
         "bias_vs_fp64_reference": metrics.bias, "rel_mse_frames": ERROR_FRAMES,
         "reference_frames": REFERENCE_FRAMES,
@@ -654,12 +691,19 @@ def own_arm(args, rank: int, world: int) -> None:
         "e2e": {"value": e2e_ms, "unit": "ms/frame", "h2d_bytes_per_step": 28, "d2h_bytes_per_step": 32,
                 "api": "restir_renderer_render + restir_renderer_measure (error record read back) per step"},
         "gpu_launches": launches * args.steps,
-        "roofline": {"bound": "hbm", "kernel": passes[dominant], "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                     "traffic": DOMINANT_TRAFFIC.get(passes[dominant]),
-                     "traffic_source": "profiles/gi_temporal_wavefront_1080p_city1M.md (ncu DRAM read+write of the "
-                                       "pass's kernels, one cold launch each)",
-                     "algorithmic_bytes_per_launch": pass_bytes[passes[dominant]]},
+        "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": DOMINANT_TRAFFIC.get(name),
+                     "traffic_source": "ncu DRAM read + write of the pass's kernels on this workload, one launch each",
+                     "algorithmic_bytes_per_launch": footprint,
+                     "algorithmic_bytes": "compulsory: the pass's image reads and writes plus each BVH row it "
+                                          "touches at most once",
+                     "fetched": {"bytes_per_launch": fetched_bytes[name], "achieved": fetched_gbs,
+                                 "peak": l2_gather_gbs, "frac": fetched_gbs / l2_gather_gbs, "unit": "GB/s",
+                                 "peak_source": "restir_gather_probe: random 32-byte gathers from the scene's BVH "
+                                                "nodes (L2-resident), measured in this run"},
+                     "limiter": "instruction issue and SIMT efficiency of divergent traversal (ncu: 9.5 of 32 "
+                                "lanes active per instruction in the queue tracer), not DRAM bandwidth"},
         "cpu_baseline": baseline,
         "clocks": clocks,
     }

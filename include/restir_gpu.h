@@ -417,7 +417,8 @@ int restir_status(uint32_t* flags);
 /* Work counters: waits for the device, returns the counts gathered since the
  * last call (8 values: nearest-hit ray casts, short-stack closest-hit rays,
  * stackless any-hit rays, depth-buffer marches, BVH node fetches, triangle
- * tests, depth-buffer steps, unused), clears them, and turns counting on or
+ * tests, depth-buffer steps, rays cut short by the step cap or a full
+ * traversal stack), clears them, and turns counting on or
  * off for the launches that follow. Off by default; a counted frame does
  * extra atomics. No counterpart in the reference (its profiler counts
  * time only, ui.cpp:20-66). */
@@ -428,6 +429,16 @@ int restir_counters(int enable, uint64_t* counters);
  * trip (restir_numeric.h), 5 unorm8 store, 6 floor(log2), 7 x^64. No
  * counterpart in the reference (a test hook). */
 int restir_numeric_eval(int fn, const float* input, float* output, uint32_t n, void* stream);
+
+/* A bandwidth probe with the traversal kernels' fetch pattern (a measurement
+ * hook, no counterpart in the reference): blocks x 256 threads each gather
+ * `gathers` rows of 32 bytes (two 16-byte read-only loads, the size of a BVH
+ * node) at seeded random indices of rows (row_count rows, 16-byte aligned)
+ * and write one float each to out (blocks x 256 floats). Fetched bytes =
+ * blocks x 256 x gathers x 32; with a buffer that fits the L2 the rate is
+ * the L2's for node-sized gathers. */
+int restir_gather_probe(const float* rows, uint32_t row_count, uint32_t blocks, uint32_t gathers, uint32_t seed,
+	float* out, void* stream);
 
 #ifdef __cplusplus
 }

@@ -89,6 +89,7 @@ _SIGNATURES = {
     "restir_status": (C.c_int, [C.POINTER(u32)]),
     "restir_numeric_eval": (C.c_int, [C.c_int, P, P, u32, P]),
     "restir_counters": (C.c_int, [C.c_int, P]),
+    "restir_gather_probe": (C.c_int, [P, u32, u32, u32, u32, P, P]),
     "restir_renderer_profile_frame": (C.c_int, [P, C.POINTER(RestirFrameInput), P]),
     "restir_renderer_pass_history": (C.c_int, [P, u32, P]),
     # restir_host.h

@@ -155,7 +155,7 @@ __device__ inline int traceStacklessWalk(const BvhView& b, V3 o, V3 d, bool anyH
 	}
 	if (step == kBvhMaxSteps)
 	{
-		raiseStatus(1u);
+		reportTruncatedRay();
 	}
 	return hit;
 }
@@ -205,7 +205,7 @@ __device__ inline int traceStacklessWave(const BvhView& b, V3 o, V3 d, bool anyH
 	}
 	if (step == kBvhMaxSteps)
 	{
-		raiseStatus(1u);
+		reportTruncatedRay();
 	}
 	return hit;
 }
@@ -275,7 +275,7 @@ __device__ inline int traceShortStack(const BvhView& b, V3 o, V3 d, float& dista
 	}
 	if (step == kBvhMaxSteps)
 	{
-		raiseStatus(1u);
+		reportTruncatedRay();
 	}
 	if (dropped)
 	{
@@ -413,7 +413,7 @@ __device__ inline int traceNearestFirst(const BvhView& b, V3 o, V3 d, float& dis
 				}
 				else
 				{
-					raiseStatus(1u);
+					reportTruncatedRay();
 				}
 				node = leftFirst ? left : right;
 				continue;

@@ -243,6 +243,7 @@ __device__ __forceinline__ void raiseStatus(unsigned int bit)
 #define RESTIR_COUNT_NODES 4
 #define RESTIR_COUNT_TRIANGLES 5
 #define RESTIR_COUNT_SCREEN_STEPS 6
+#define RESTIR_COUNT_STEP_CAPPED 7  // rays cut short: the step cap, or a full traversal stack
 #define RESTIR_COUNTERS 8
 
 extern __device__ unsigned long long g_restirCounters[RESTIR_COUNTERS];
@@ -266,6 +267,17 @@ __device__ __forceinline__ void countWork(int kind, uint32_t nodes, uint32_t tri
 		{
 			atomicAdd(&g_restirCounters[RESTIR_COUNT_TRIANGLES], static_cast<unsigned long long>(t));
 		}
+	}
+}
+
+// A traversal stopped short (the 2,048-visit cap, bvh.sh:23, or a full
+// traversal stack): status bit 0, and one ray counted while counting is on.
+__device__ __forceinline__ void reportTruncatedRay()
+{
+	raiseStatus(1u);
+	if (g_restirCounting)
+	{
+		atomicAdd(&g_restirCounters[RESTIR_COUNT_STEP_CAPPED], 1ull);
 	}
 }
 

@@ -124,7 +124,7 @@ __device__ __forceinline__ void endShortStack(ShortStackState& s)
 {
 	if (s.step == kBvhMaxSteps)
 	{
-		raiseStatus(1u);
+		reportTruncatedRay();
 	}
 	if (s.dropped)
 	{
@@ -151,7 +151,7 @@ __device__ __forceinline__ void stepStacklessWalk(ShortStackState& s, const BvhV
 	{
 		if (s.step >= kBvhMaxSteps)
 		{
-			raiseStatus(1u);
+			reportTruncatedRay();
 		}
 		if (s.fallbackHit >= 0)
 		{
