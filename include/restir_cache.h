@@ -92,7 +92,10 @@ typedef struct RestirCacheLayout
 	uint64_t table_half;      /* uint16 copy the queries read */
 	uint64_t table_m;
 	uint64_t table_v;
-	uint64_t table_grad;      /* float, scaled by the loss scale while accumulating */
+	uint64_t table_grad;      /* float, the last gradient (unscaled) */
+	uint64_t table_grad_fixed; /* int64, the loss-scaled gradient summed in units of 2^-32
+	                              (fixed point: the sum does not depend on the order of the
+	                              samples' scattered contributions) */
 	uint64_t scalars;         /* RestirCacheScalars */
 	uint64_t bytes;           /* total */
 	uint32_t entries;         /* per level */

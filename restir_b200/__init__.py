@@ -530,7 +530,7 @@ class RadianceCache:
         offset = getattr(self.layout, name)
         itemsize = torch.empty((), dtype=dtype).element_size()
         if count is None:
-            ends = sorted(getattr(self.layout, f) for f, _ in abi.RestirCacheLayout._fields_[:13])
+            ends = sorted(getattr(self.layout, f) for f, _ in abi.RestirCacheLayout._fields_[:14])
             count = (ends[ends.index(offset) + 1] - offset) // itemsize
         return self.state[offset:offset + count * itemsize].view(dtype)
 

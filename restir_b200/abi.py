@@ -177,7 +177,7 @@ class RestirCacheLayout(C.Structure):
         ("weights", C.c_uint64), ("weights_bf16", C.c_uint64), ("weight_m", C.c_uint64), ("weight_v", C.c_uint64),
         ("weight_grad", C.c_uint64), ("weight_partials", C.c_uint64), ("table", C.c_uint64),
         ("table_half", C.c_uint64), ("table_m", C.c_uint64), ("table_v", C.c_uint64), ("table_grad", C.c_uint64),
-        ("scalars", C.c_uint64), ("bytes", C.c_uint64), ("entries", C.c_uint32), ("partial_blocks", C.c_uint32),
+        ("table_grad_fixed", C.c_uint64), ("scalars", C.c_uint64), ("bytes", C.c_uint64), ("entries", C.c_uint32), ("partial_blocks", C.c_uint32),
         ("level_scale", C.c_float * CACHE_LEVELS), ("level_dense", C.c_uint32 * CACHE_LEVELS),
     ]
 

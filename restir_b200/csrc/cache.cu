@@ -489,9 +489,30 @@ struct TrainArgs
 	const float4* targets;
 	uint32_t n;
 	const float* scalars;   // RestirCacheScalars: loss_scale first
+	uint32_t* nonfinite;    // RestirCacheScalars::nonfinite
 	float* partials;        // [blocks][RESTIR_CACHE_PARTIAL_STRIDE]
-	float* tableGrad;
+	unsigned long long* tableGradFixed; // the table gradient in fixed point (kGradientFixedScale)
 };
+
+// The hash table's gradient is summed in 64-bit fixed point, units of 2^-32
+// of the loss-scaled gradient: integer addition is associative, so the sum
+// of the samples' scattered contributions does not depend on the order the
+// atomics land in, and a training step is reproducible bit for bit. One
+// contribution of magnitude 2^20 or more (or not finite) marks the step
+// non-finite instead (the loss-scale logic then halves the scale and skips
+// it); a sum stays within range below 2^11 such contributions per entry.
+constexpr float kGradientFixedScale = 4294967296.0f; // 2^32
+constexpr float kGradientFixedLimit = 1048576.0f;    // 2^20
+
+__device__ __forceinline__ void scatterFixed(unsigned long long* target, float value, bool& overflow)
+{
+	if (!(fabsf(value) < kGradientFixedLimit))
+	{
+		overflow = true;
+		return;
+	}
+	atomicAdd(target, static_cast<unsigned long long>(__float2ll_rn(value * kGradientFixedScale)));
+}
 
 __global__ void __launch_bounds__(kTile, 1) trainKernel(TrainArgs a)
 {
@@ -688,16 +709,22 @@ __global__ void __launch_bounds__(kTile, 1) trainKernel(TrainArgs a)
 				}
 				float unit[3];
 				unitPosition(a.c, a.queries[size_t(row) * 4], unit);
+				bool overflow = false;
 				for (int level = 0; level < RESTIR_CACHE_LEVELS; ++level)
 				{
 					LevelCorners corners;
 					levelCorners(a.c, level, unit, corners);
-					float* grad = a.tableGrad + (size_t(level) * a.c.entries) * 2;
+					unsigned long long* grad = a.tableGradFixed + (size_t(level) * a.c.entries) * 2;
 					for (int d = 0; d < 8; ++d)
 					{
-						atomicAdd(grad + size_t(corners.index[d]) * 2, corners.weight[d] * dx[2 * level]);
-						atomicAdd(grad + size_t(corners.index[d]) * 2 + 1, corners.weight[d] * dx[2 * level + 1]);
+						scatterFixed(grad + size_t(corners.index[d]) * 2, corners.weight[d] * dx[2 * level], overflow);
+						scatterFixed(grad + size_t(corners.index[d]) * 2 + 1, corners.weight[d] * dx[2 * level + 1],
+							overflow);
 					}
+				}
+				if (overflow)
+				{
+					atomicOr(a.nonfinite, 1u);
 				}
 			}
 		}
@@ -766,6 +793,7 @@ struct StepArgs
 	float* tableM;
 	float* tableV;
 	float* tableGrad;
+	unsigned long long* tableGradFixed;
 	RestirCacheScalars* scalars;
 	uint32_t tableCount;
 	float learningRate, beta1, beta2, epsilon;
@@ -777,7 +805,8 @@ __device__ __forceinline__ bool finite(float x)
 }
 
 // Weight gradients: the blocks' partial rows summed in block order, unscaled;
-// the table gradient unscaled in place; the non-finite flag; the mean loss.
+// the table gradient converted from its fixed-point sum and unscaled; the
+// non-finite flag; the mean loss.
 __global__ void reduceKernel(StepArgs s, uint32_t blocks, uint32_t samples)
 {
 	const float inverseScale = 1.0f / s.scalars->loss_scale;
@@ -799,7 +828,8 @@ __global__ void reduceKernel(StepArgs s, uint32_t blocks, uint32_t samples)
 		else
 		{
 			const uint32_t j = i - RESTIR_CACHE_WEIGHTS;
-			const float g = s.tableGrad[j] * inverseScale;
+			const long long fixed = static_cast<long long>(s.tableGradFixed[j]);
+			const float g = float(double(fixed) * (1.0 / double(kGradientFixedScale))) * inverseScale;
 			s.tableGrad[j] = g;
 			bad = bad || !finite(g);
 		}
@@ -939,6 +969,7 @@ __global__ void initKernel(StepArgs s, uint32_t seed, float initialLossScale)
 			s.tableM[j] = 0.0f;
 			s.tableV[j] = 0.0f;
 			s.tableGrad[j] = 0.0f;
+			s.tableGradFixed[j] = 0ull;
 		}
 	}
 	if (blockIdx.x == 0 && threadIdx.x == 0)
@@ -966,6 +997,7 @@ StepArgs stepArgs(const RestirCacheConfig& cfg, const RestirCacheLayout& l, void
 	s.tableM = reinterpret_cast<float*>(base + l.table_m);
 	s.tableV = reinterpret_cast<float*>(base + l.table_v);
 	s.tableGrad = reinterpret_cast<float*>(base + l.table_grad);
+	s.tableGradFixed = reinterpret_cast<unsigned long long*>(base + l.table_grad_fixed);
 	s.scalars = reinterpret_cast<RestirCacheScalars*>(base + l.scalars);
 	s.tableCount = uint32_t(RESTIR_CACHE_LEVELS) * l.entries * RESTIR_CACHE_FEATURES;
 	s.learningRate = cfg.learning_rate;
@@ -1071,7 +1103,7 @@ extern "C" int restir_cache_gradients(const RestirCacheConfig* cfg, void* state,
 	}
 	StepArgs s = stepArgs(*cfg, l, state);
 	cudaStream_t st = asStream(stream);
-	cudaMemsetAsync(s.tableGrad, 0, size_t(s.tableCount) * 4, st);
+	cudaMemsetAsync(s.tableGradFixed, 0, size_t(s.tableCount) * 8, st);
 	const uint32_t tiles = (n + kTile - 1) / kTile;
 	const uint32_t blocks = n == 0u ? 0u : min(tiles, min(uint32_t(smCount()), l.partial_blocks));
 	if (blocks > 0u)
@@ -1089,7 +1121,8 @@ extern "C" int restir_cache_gradients(const RestirCacheConfig* cfg, void* state,
 		a.n = n;
 		a.scalars = reinterpret_cast<const float*>(s.scalars);
 		a.partials = reinterpret_cast<float*>(static_cast<char*>(state) + l.weight_partials);
-		a.tableGrad = s.tableGrad;
+		a.tableGradFixed = s.tableGradFixed;
+		a.nonfinite = &s.scalars->nonfinite;
 		trainKernel<<<blocks, kTile, kTrainSmem, st>>>(a);
 	}
 	reduceKernel<<<smCount() * 4, 256, 0, st>>>(s, blocks, n);

@@ -79,6 +79,7 @@ extern "C" int restir_cache_layout(const RestirCacheConfig* cfg, RestirCacheLayo
 	l.table_m = take(table * 4);
 	l.table_v = take(table * 4);
 	l.table_grad = take(table * 4);
+	l.table_grad_fixed = take(table * 8);
 	l.scalars = take(sizeof(RestirCacheScalars));
 	l.bytes = at;
 	// Level l at floor(n_min * b^l) cells across the box, b the growth factor

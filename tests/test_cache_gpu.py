@@ -230,3 +230,28 @@ def test_renderer_cache_forms_train_on_a_side_stream(cache_only):
     raw = rb.device_view(pointer, nbytes, torch.uint8)[layout.scalars:layout.scalars + 64].cpu().numpy()
     scalars = rb.abi.RestirCacheScalars.from_buffer_copy(raw[:C.sizeof(rb.abi.RestirCacheScalars)].tobytes())
     assert scalars.step == 6
+
+
+@pytest.mark.gpu
+def test_training_is_reproducible_bit_for_bit():
+    """Two caches from the same seed, trained on the same batches, stay equal
+    bit for bit: the weight gradients are summed in block order and the hash
+    table's gradient in 64-bit fixed point, so no step depends on the order in
+    which the samples' scattered contributions arrive (a 4,096-entry table
+    and 65,536 samples give every entry many colliding contributions)."""
+    import torch
+    caches = [small_cache(), small_cache()]
+    q = make_queries(65536, seed=11)
+    t = target_function(q)
+    dq, dt = torch.from_numpy(q).cuda(), torch.from_numpy(t).cuda()
+    for step in range(25):
+        for cache in caches:
+            cache.train(dq, dt)
+        if step in (0, 24):
+            torch.cuda.synchronize()
+            for name in ("table_grad", "weight_grad", "table", "weights"):
+                a = host_region(caches[0], name, torch.int32)
+                b = host_region(caches[1], name, torch.int32)
+                assert np.array_equal(a, b), (step, name)
+    assert caches[0].scalars().skipped_steps == 0
+    assert np.count_nonzero(host_region(caches[0], "table_grad", torch.float32)) > 1000
