@@ -44,8 +44,10 @@ METRIC = "1080p ms/frame at equal relMSE vs FP64 ref: plain vs radiance-cache; M
 WIDTH, HEIGHT = 1920, 1080
 TRIANGLES = 1_000_000
 EXTRA_LIGHTS = 64
-REFERENCE_FRAMES = 64
-ERROR_FRAMES = 240         # frames the relMSE is averaged over (it swings by +-0.07 between 30-frame windows)
+# The FP64 reference of the view: 1,024 frames (a 64-frame reference of this many-light view is far from
+# converged: two 32-frame halves differ by a relative MSE of 30, which swamps the method's own error).
+REFERENCE_FRAMES = 1024
+ERROR_FRAMES = 120         # frames the relMSE and bias are averaged over
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per frame of the GI temporal pass's
 # three kernels on this workload, one launch each, captured from the current build.
 DOMINANT_TRAFFIC = {"gi_temporal": 134.9e6}
@@ -104,6 +106,31 @@ def gather_probe(renderer, repeats: int = 5) -> float:
     torch.cuda.synchronize()
     fetched = blocks * 256 * gathers * 32 * repeats
     return fetched / (start.elapsed_time(stop) * 1e-3) / 1e9
+
+
+def accumulate_reference(renderer, frame, frames: int = REFERENCE_FRAMES) -> dict:
+    """The FP64 progressive reference of the view (reference mode, `frames`
+    frames), and its own noise: the relative MSE and bias between its two
+    halves (frames 1..n/2 and n/2+1..n), each a reference of n/2 frames;
+    the whole reference's error against the converged image is about a
+    quarter of that relative MSE."""
+    n = frame.width * frame.height
+    renderer.set_reference_accumulation(True)
+    half = None
+    for i in range(frames):
+        renderer.render(frame)
+        if i + 1 == frames // 2:
+            half = renderer.download("reference.mean", np.float64)[:3 * n].copy()
+    full = renderer.download("reference.mean", np.float64)[:3 * n].copy()
+    alpha = renderer.download("reference.alpha", np.uint8)[:n] > 0
+    renderer.set_reference_accumulation(False)
+    second = 2.0 * full - half
+
+    def luminance(mean):
+        return 0.2126 * mean[:n] + 0.7152 * mean[n:2 * n] + 0.0722 * mean[2 * n:]
+    a, b = luminance(half)[alpha], luminance(second)[alpha]
+    return {"frames": frames, "split_half_rel_mse": float(np.mean((a - b) ** 2 / (b * b + 0.01))),
+            "split_half_bias": float(a.mean() / b.mean() - 1.0)}
 
 
 def load_peaks() -> tuple[float, str]:
@@ -353,10 +380,7 @@ def pareto(args) -> None:
                 continue
             renderer = rb.Renderer(settings)
             renderer.set_scene(mesh)
-            renderer.set_reference_accumulation(True)
-            for _ in range(REFERENCE_FRAMES):
-                renderer.render(frame)
-            renderer.set_reference_accumulation(False)
+            accumulate_reference(renderer, frame)
             s = renderer.settings
             for field, value in changes.items():
                 setattr(s, field, value)
@@ -460,11 +484,13 @@ def max_over_ranks(values, dist, device: str) -> list:
 
 def error_stats(renderer, frame, frames: int) -> dict:
     """relMSE of the live image against the FP64 reference over `frames` frames."""
-    values = []
+    values, biases = [], []
     for _ in range(frames):
         renderer.render(frame)
-        values.append(renderer.frame_submitted().relative_mse)
-    return {"mean": float(np.mean(values)), "median": float(np.median(values))}
+        metrics = renderer.frame_submitted()
+        values.append(metrics.relative_mse)
+        biases.append(metrics.bias)
+    return {"mean": float(np.mean(values)), "median": float(np.median(values)), "bias": float(np.mean(biases))}
 
 
 def cache_arm(renderer, frame, steps: int, changes: dict | None = None) -> dict:
@@ -501,7 +527,8 @@ def cache_arm(renderer, frame, steps: int, changes: dict | None = None) -> dict:
     for name, value in saved.items():
         setattr(settings, name, value)
     renderer.settings = settings
-    return {"ms_per_frame": ms, "settings": dict(changes or {}), "rel_mse_vs_fp64_reference": error["mean"], "rel_mse_median": error["median"],
+    return {"ms_per_frame": ms, "settings": dict(changes or {}), "rel_mse_vs_fp64_reference": error["mean"],
+            "rel_mse_median": error["median"], "bias_vs_fp64_reference": error["bias"],
             "training_frames": CACHE_TRAIN_FRAMES + steps, "training_samples_per_frame": int(params.cache_training_samples),
             "pass_ms": {name: float(mean_pass[i]) for i, name in enumerate(rb.PASS_NAMES)}}
 
@@ -550,10 +577,7 @@ def own_arm(args, rank: int, world: int) -> None:
         return
 
     # FP64 progressive reference of this view (not timed).
-    renderer.set_reference_accumulation(True)
-    for _ in range(REFERENCE_FRAMES):
-        renderer.render(frame)
-    renderer.set_reference_accumulation(False)
+    reference = accumulate_reference(renderer, frame)
 
     # Let the live history settle, then one profiling frame for the work counts.
     for _ in range(max(args.warmup, 3)):
@@ -671,8 +695,8 @@ def own_arm(args, rank: int, world: int) -> None:
         "depth_buffer_marches_per_frame": int(counts[:, 3].sum()),
         "truncated_rays_per_frame": int(counts[:, 7].sum()),
         "rel_mse_vs_fp64_reference": plain_error["mean"], "rel_mse_median": plain_error["median"],
-        "bias_vs_fp64_reference": metrics.bias, "rel_mse_frames": ERROR_FRAMES,
-        "reference_frames": REFERENCE_FRAMES,
+        "bias_vs_fp64_reference": plain_error["bias"], "rel_mse_frames": ERROR_FRAMES,
+        "reference_frames": REFERENCE_FRAMES, "reference_noise": reference,
         "radiance_cache": cache_line,
         "radiance_cache_only_gi": cache_only_line,
         # The metric's comparison: plain ms/frame over the cache-only form's, when the
