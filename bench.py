@@ -353,6 +353,8 @@ PARETO_VARIANTS = [
     # the cache-only GI (no GI rays: the cache at each GI pixel's surface); radiance-cache form only
     ("cache_only", {"cache_only_gi": 1}),
     ("cache_only_no_specular", {"cache_only_gi": 1, "specular_gi": 0}),
+    ("cache_only_more_training", {"cache_only_gi": 1, "cache_training_samples": 131072}),
+    ("cache_only_lr3e-3", {"cache_only_gi": 1, "cache_learning_rate": 3e-3}),
     # diagnostic: no indirect light at all (how much of the error the GI term carries)
     ("no_gi", {"initial_candidates": 0, "temporal_taps": 0, "spatial_taps": 0, "specular_gi": 0}),
 ]
@@ -417,6 +419,138 @@ def settings_fields(settings):
 
 
 BATCH_SIZES = [(640, 360), (960, 540), (1280, 720), (1920, 1080), (800, 450), (1600, 900), (1024, 576), (1440, 810)]
+
+
+def camera_path(rb, mesh, width: int, height: int, frames: int, seed: int = 0):
+    """A seeded camera path: the eye moves through four seeded control points
+    around the scene's default view (Catmull-Rom), yaw and pitch sway with
+    it; one frame input per frame at 1/60 s."""
+    rng = np.random.default_rng(seed)
+    radius = mesh.desc.radius
+    eye0 = np.array(mesh.desc.camera_eye, np.float64)
+    points = eye0 + rng.uniform(-0.08, 0.08, (4, 3)) * radius
+    points[:, 1] = eye0[1] + rng.uniform(-0.02, 0.04, 4) * radius
+    yaws = mesh.desc.camera_yaw + rng.uniform(-0.25, 0.25, 4)
+    pitches = mesh.desc.camera_pitch + rng.uniform(-0.05, 0.05, 4)
+    inputs = []
+    for i in range(frames):
+        t = 3.0 * i / max(frames - 1, 1)
+        k = min(int(t), 2)
+        u = t - k
+
+        def spline(v):
+            p0, p1, p2, p3 = v[max(k - 1, 0)], v[k], v[k + 1], v[min(k + 2, 3)]
+            return 0.5 * ((2 * p1) + (-p0 + p2) * u + (2 * p0 - 5 * p1 + 4 * p2 - p3) * u * u
+                          + (-p0 + 3 * p1 - 3 * p2 + p3) * u ** 3)
+        inputs.append(rb.frame_input(mesh, width, height, eye=[float(x) for x in spline(points)],
+                                     yaw=float(spline(yaws)), pitch=float(spline(pitches))))
+    return inputs
+
+
+def mid_config(args) -> None:
+    """--config mid: the mid configuration, a seeded courtyard of instanced boxes
+    and arches (100k triangles, albedo U[0.2, 0.8], roughness U[0.05, 1]) with
+    64 extra point lights beside its 256 emissive triangles, 1280x720, GI at
+    half resolution with temporal and spatial reuse, ReSTIR DI, SVGF with 5
+    a-trous levels, a 2^20-slot hash grid, 60 frames on a seeded camera path
+    (device time per frame, CUDA events). Then, held at the path's last pose,
+    the relative MSE and bias against a 1,024-frame FP64 reference."""
+    import torch
+    import restir_b200 as rb
+    mesh = rb.Mesh.procedural(rb.SCENE_COURTYARD, 0, 100_000)
+    renderer = rb.Renderer(rb.default_settings(mesh))
+    renderer.set_scene(mesh, use_scene_defaults=True)
+    settings = renderer.settings
+    settings.extra_lights = 64
+    settings.grid_table_size = 1 << 20
+    renderer.settings = settings
+    path = camera_path(rb, mesh, 1280, 720, 60)
+    for _ in range(args.warmup):
+        renderer.render(path[0])
+    stream = torch.cuda.ExternalStream(renderer.stream)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record(stream)
+    for frame in path:
+        renderer.render(frame)
+    stop.record(stream)
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(stop) / len(path)
+    pass_ms = renderer.pass_history(len(path)).mean(axis=0)
+    final = path[-1]
+    counts = renderer.profile_frame(final)
+    reference = accumulate_reference(renderer, final)
+    for _ in range(60):
+        renderer.render(final)
+    error = error_stats(renderer, final, 60)
+    params, _, _ = renderer.last_frame()
+    rays = int(counts[:, 0:3].sum())
+    print(json.dumps({"config": "mid", "workload": "1280x720, seeded 100k-triangle courtyard, 64 point lights + "
+                      "256 emissive triangles, GI 1/2 res + DI + specular GI + SVGF x5 + TAA, 2^20-slot grid, "
+                      "60-frame seeded camera path", "scene_triangles": mesh.triangle_count,
+                      "di_lights": params.di_light_count, "grid_table_size": params.grid_table_size,
+                      "ms_per_frame": ms, "frames": len(path), "mrays_per_s": rays / (ms * 1e-3) / 1e6,
+                      "rel_mse_vs_fp64_reference": error["mean"], "bias_vs_fp64_reference": error["bias"],
+                      "reference_noise": reference, "truncated_rays_per_frame": int(counts[:, 7].sum()),
+                      "pass_ms": {name: float(pass_ms[i]) for i, name in enumerate(rb.PASS_NAMES)},
+                      "status": rb.status_flags()}), flush=True)
+    renderer.close()
+
+
+def stress_config(args) -> None:
+    """--config stress: the stress configuration, 3840x2160 on the seeded
+    4M-triangle city with 2,048 emissive panels (4,096 emissive triangles) and
+    1,024 extra point lights orbiting on seeded circles, GI + DI + SVGF + the
+    radiance cache (GI passes with the cache), a 2^22-slot hash grid, 240
+    frames at 1/60 s (device time per frame, CUDA events). Then, with the
+    lights held where they are (delta_time 0), the relative MSE and bias
+    against a 4,096-frame FP64 reference (4,096 samples per pixel)."""
+    import torch
+    import restir_b200 as rb
+    mesh = rb.Mesh.procedural(rb.SCENE_CITY_LIT, 0, 4_000_000)
+    renderer = rb.Renderer(rb.default_settings(mesh))
+    t = time.perf_counter()
+    renderer.set_scene(mesh, use_scene_defaults=True)
+    scene_ms = (time.perf_counter() - t) * 1e3
+    settings = renderer.settings
+    settings.extra_lights = 1024
+    settings.grid_table_size = 1 << 22
+    settings.radiance_cache = 1
+    settings.extra_light_orbit = 0.5
+    renderer.settings = settings
+    frame = rb.frame_input(mesh, 3840, 2160)
+    for _ in range(max(args.warmup, 3)):
+        renderer.render(frame)
+    stream = torch.cuda.ExternalStream(renderer.stream)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    frames = 240
+    torch.cuda.synchronize()
+    start.record(stream)
+    for _ in range(frames):
+        renderer.render(frame)
+    stop.record(stream)
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(stop) / frames
+    pass_ms = renderer.pass_history(min(frames, 64)).mean(axis=0)
+    held = rb.frame_input(mesh, 3840, 2160, delta_time=0.0)
+    counts = renderer.profile_frame(held)
+    reference = accumulate_reference(renderer, held, 4096)
+    for _ in range(120):
+        renderer.render(held)
+    error = error_stats(renderer, held, 60)
+    params, _, _ = renderer.last_frame()
+    rays = int(counts[:, 0:3].sum())
+    print(json.dumps({"config": "stress", "workload": "3840x2160, seeded 4M-triangle city, 1,024 orbiting point "
+                      "lights + 4,096 emissive triangles, GI 1/2 res with the radiance cache + DI + specular GI + "
+                      "SVGF x5 + TAA, 2^22-slot grid, 240 frames", "scene_triangles": mesh.triangle_count,
+                      "scene_setup_ms": scene_ms, "di_lights": params.di_light_count,
+                      "grid_table_size": params.grid_table_size, "ms_per_frame": ms, "frames": frames,
+                      "mrays_per_s": rays / (ms * 1e-3) / 1e6, "rel_mse_vs_fp64_reference": error["mean"],
+                      "bias_vs_fp64_reference": error["bias"], "reference_noise": reference,
+                      "truncated_rays_per_frame": int(counts[:, 7].sum()),
+                      "pass_ms": {name: float(pass_ms[i]) for i, name in enumerate(rb.PASS_NAMES)},
+                      "status": rb.status_flags()}), flush=True)
+    renderer.close()
 
 
 def batched(args) -> None:
@@ -746,6 +880,9 @@ def main():
     parser.add_argument("--graph", action="store_true", help="replay each frame as a CUDA graph")
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--no-cache", action="store_true", help="skip the radiance-cache form's measurement")
+    parser.add_argument("--config", choices=["mid", "stress"], default=None,
+                        help="another configuration of the metric's family (mid: 720p courtyard on a camera path; "
+                             "stress: 4K, 4M triangles, 1,024 orbiting lights)")
     parser.add_argument("--batched", action="store_true",
                         help="the batched multi-view form (8 views of uneven resolution in one frame)")
     parser.add_argument("--cache-kernels", action="store_true",
@@ -769,6 +906,10 @@ def main():
         bvh_build(args)
     elif args.pareto:
         pareto(args)
+    elif args.config == "mid":
+        mid_config(args)
+    elif args.config == "stress":
+        stress_config(args)
     elif args.batched:
         batched(args)
     elif args.impl == "reference":

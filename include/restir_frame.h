@@ -84,6 +84,12 @@ typedef struct RestirSettings
 	                            rays, no reuse, no denoiser */
 	float cache_learning_rate; /* no reference counterpart: the cache's Adam step size
 	                              (0: restir_cache_config_default's) */
+	float extra_light_orbit;   /* no reference counterpart (the reference orbits only its
+	                              main light, main.cpp:505-518): > 0 moves every extra point
+	                              light on a horizontal circle about the scene's vertical
+	                              axis, light i at extra_light_orbit * s_i radians per
+	                              second of RestirFrameInput::delta_time, s_i a seeded speed
+	                              in [-1, -0.25] or [0.25, 1]; the list is uploaded per frame */
 } RestirSettings;
 
 /* FrameInput (renderer.h) with the fly camera's pose. */

@@ -25,6 +25,8 @@ extern "C" {
 #define RESTIR_SCENE_CORNELL 0   /* open-front Cornell box, 36 triangles */
 #define RESTIR_SCENE_COURTYARD 1 /* seeded boxes and arches, ~target triangles */
 #define RESTIR_SCENE_CITY 2      /* seeded boxes, 512-triangle spheres, thin planes */
+#define RESTIR_SCENE_CITY_LIT 3  /* the city with 2,048 emissive panels (4,096 emissive triangles)
+                                    instead of 128: the stress configuration's scene */
 
 /* A triangle soup with one material per triangle. Materials: 8 floats each,
  * (base colour rgb, roughness), (emission rgb, metallic). */

@@ -513,6 +513,9 @@ void* oracle_mesh_procedural(int kind, uint32_t seed, uint32_t target_triangles)
 	case RESTIR_SCENE_CITY:
 		*mesh = restir::makeCity(seed, target_triangles);
 		break;
+	case RESTIR_SCENE_CITY_LIT:
+		*mesh = restir::makeCity(seed, target_triangles, 2048);
+		break;
 	default:
 		delete mesh;
 		return nullptr;

@@ -26,7 +26,7 @@ from .abi import (RestirBvhDesc, RestirDiReservoirs, RestirFrameInput, RestirFra
 # RESTIR_LIBRARY selects another build of the same library (tuning variants).
 LIBRARY_PATH = Path(os.environ.get("RESTIR_LIBRARY", Path(__file__).resolve().parent / "librestir_gpu.so"))
 
-SCENE_CORNELL, SCENE_COURTYARD, SCENE_CITY = 0, 1, 2
+SCENE_CORNELL, SCENE_COURTYARD, SCENE_CITY, SCENE_CITY_LIT = 0, 1, 2, 3
 GRID_ATOMIC, GRID_DETERMINISTIC = 0, 1
 RAY_SCREEN, RAY_HYBRID, RAY_BVH = 0, 1, 2
 # restir_gpu.h status codes

@@ -108,6 +108,7 @@ class RestirSettings(C.Structure):
         ("taa", C.c_int), ("auto_exposure", C.c_int), ("tonemapper", C.c_int), ("exposure_ev", C.c_float),
         ("adaptation_speed", C.c_float), ("display", C.c_int), ("bvh_on_device", C.c_int), ("specular_gi", C.c_int),
         ("cache_only_gi", C.c_int), ("cache_learning_rate", C.c_float),
+        ("extra_light_orbit", C.c_float),
     ]
 
 

@@ -56,23 +56,30 @@ def _run(command: list[str]) -> None:
         raise RuntimeError("build failed:\n" + " ".join(command) + "\n" + result.stdout + result.stderr)
 
 
+FAST_LIBRARY = PACKAGE / "librestir_gpu_fast.so"
+
+
 def build(verbose: bool = False, defines: list[str] | None = None, library: Path = LIBRARY,
-          objects_dir: Path = BUILD) -> Path:
+          objects_dir: Path = BUILD, contract: bool = False) -> Path:
     """Compiles stale objects and links the library. defines: extra -D macros for
     the CUDA sources (tuning knobs such as RESTIR_GI_TEMPORAL_MIN_BLOCKS=4),
-    built into their own objects_dir and library."""
+    built into their own objects_dir and library. contract: the kernels with
+    FMA contraction (--fmad=true), a measurement variant that leaves the
+    parity conventions of include/restir_numeric.h (its results differ from
+    the oracle's in the last bits)."""
     objects_dir = Path(objects_dir)
     objects_dir.mkdir(parents=True, exist_ok=True)
     nvcc = _nvcc()
     headers = _headers()
     extra = [f"-D{d}" for d in (defines or [])]
+    nvcc_flags = [("--fmad=true" if f == "--fmad=false" else f) for f in NVCC_FLAGS] if contract else NVCC_FLAGS
     jobs = []
     objects = []
     for source in sorted(CSRC.glob("*.cu")):
         obj = objects_dir / (source.stem + ".cu.o")
         objects.append(obj)
         if _stale(obj, [source] + headers):
-            jobs.append([nvcc] + NVCC_FLAGS + extra + ["-c", str(source), "-o", str(obj)])
+            jobs.append([nvcc] + nvcc_flags + extra + ["-c", str(source), "-o", str(obj)])
     for source in sorted(HOST.glob("*.cpp")):
         obj = objects_dir / (source.stem + ".cpp.o")
         objects.append(obj)
@@ -92,4 +99,8 @@ def build(verbose: bool = False, defines: list[str] | None = None, library: Path
 
 
 if __name__ == "__main__":
-    print(build(verbose="-v" in sys.argv))
+    if "--contract" in sys.argv:
+        print(build(verbose="-v" in sys.argv, library=FAST_LIBRARY, objects_dir=BUILD.parent / "_build_contract",
+                    contract=True))
+    else:
+        print(build(verbose="-v" in sys.argv))

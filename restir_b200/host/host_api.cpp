@@ -41,6 +41,9 @@ extern "C" void* restir_mesh_procedural(int kind, uint32_t seed, uint32_t target
 	case RESTIR_SCENE_CITY:
 		*mesh = makeCity(seed, target_triangles);
 		break;
+	case RESTIR_SCENE_CITY_LIT:
+		*mesh = makeCity(seed, target_triangles, 2048);
+		break;
 	default:
 		delete mesh;
 		return nullptr;

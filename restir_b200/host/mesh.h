@@ -44,7 +44,7 @@ struct Mesh
 
 Mesh makeCornell();
 Mesh makeCourtyard(uint32_t seed, uint32_t targetTriangles);
-Mesh makeCity(uint32_t seed, uint32_t targetTriangles);
+Mesh makeCity(uint32_t seed, uint32_t targetTriangles, int emissivePanelCount = 128);
 
 // A small deterministic generator (the PCG output function of lights.cpp:15-26).
 struct Random

@@ -15,6 +15,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -99,6 +100,10 @@ public:
 			}
 		}
 		cudaMallocHost(&m_errorHost, 4 * sizeof(double));
+		for (int k = 0; k < 2; ++k)
+		{
+			cudaEventCreateWithFlags(&m_orbitCopied[k], cudaEventDisableTiming);
+		}
 	}
 
 	~Renderer()
@@ -116,6 +121,11 @@ public:
 			}
 		}
 		cudaFreeHost(m_errorHost);
+		for (int k = 0; k < 2; ++k)
+		{
+			cudaEventDestroy(m_orbitCopied[k]);
+			cudaFreeHost(m_orbitHost[k]);
+		}
 		cudaStreamSynchronize(m_side);
 		cudaEventDestroy(m_fork);
 		cudaEventDestroy(m_join);
@@ -221,6 +231,10 @@ public:
 			return RESTIR_ERROR_INVALID_ARGUMENT;
 		}
 		int status = updateLights();
+		if (status == RESTIR_OK)
+		{
+			status = orbitLights(input.delta_time);
+		}
 		if (status != RESTIR_OK)
 		{
 			return status;
@@ -590,6 +604,62 @@ private:
 		m_state.di_valid = 0; // stored light indices refer to the old list
 		releaseGraph();
 		return status == 0 ? RESTIR_OK : RESTIR_ERROR_OUT_OF_MEMORY;
+	}
+
+	// The extra point lights on their orbits (RestirSettings::extra_light_orbit):
+	// light k turns about the vertical axis through the scene's centre by
+	// orbit * s_k * t radians, t the frames' accumulated delta_time, s_k a
+	// seeded speed in [0.25, 1] with a seeded sign. The moved list is written
+	// to one of two pinned host buffers (the other may still be copying) and
+	// copied to the device on the frame's stream.
+	int orbitLights(float deltaTime)
+	{
+		const LightListResult& list = m_scene->lights;
+		if (!(m_settings.extra_light_orbit > 0.0f) || list.count == list.triangles)
+		{
+			return RESTIR_OK;
+		}
+		m_orbitTime += double(deltaTime);
+		const size_t floats = size_t(list.count) * 16u;
+		const int k = m_orbitSlot;
+		m_orbitSlot ^= 1;
+		if (m_orbitCapacity[k] < floats)
+		{
+			cudaEventSynchronize(m_orbitCopied[k]);
+			cudaFreeHost(m_orbitHost[k]);
+			m_orbitHost[k] = nullptr;
+			m_orbitCapacity[k] = 0;
+			if (cudaMallocHost(reinterpret_cast<void**>(&m_orbitHost[k]), floats * sizeof(float)) != cudaSuccess)
+			{
+				return RESTIR_ERROR_OUT_OF_MEMORY;
+			}
+			m_orbitCapacity[k] = floats;
+		}
+		// The copy this buffer fed two frames ago has finished before it is rewritten.
+		cudaEventSynchronize(m_orbitCopied[k]);
+		float* out = m_orbitHost[k];
+		std::memcpy(out, list.data.data(), floats * sizeof(float));
+		const float cx = m_scene->mesh.center[0], cz = m_scene->mesh.center[2];
+		for (uint32_t light = list.triangles; light < list.count; ++light)
+		{
+			uint32_t h = uint32_t(light - list.triangles) * 2654435761u + uint32_t(m_settings.extra_seed) * 97u + 1u;
+			h = h * 747796405u + 2891336453u;
+			h = ((h >> ((h >> 28u) + 4u)) ^ h) * 277803737u;
+			h = (h >> 22u) ^ h;
+			const float speed = (0.25f + 0.75f * float(h >> 8) * (1.0f / 16777216.0f)) * ((h & 1u) ? 1.0f : -1.0f);
+			const double angle = double(m_settings.extra_light_orbit) * double(speed) * m_orbitTime;
+			const float c = float(std::cos(angle)), sn = float(std::sin(angle));
+			float* row = out + size_t(light) * 16u;
+			const float dx = row[0] - cx, dz = row[2] - cz;
+			row[0] = cx + c * dx + sn * dz;
+			row[2] = cz - sn * dx + c * dz;
+		}
+		if (cudaMemcpyAsync(m_scene->buffers["lights"].pointer, out, floats * sizeof(float), cudaMemcpyHostToDevice,
+				m_stream) != cudaSuccess || cudaEventRecord(m_orbitCopied[k], m_stream) != cudaSuccess)
+		{
+			return RESTIR_ERROR_LAUNCH;
+		}
+		return RESTIR_OK;
 	}
 
 	// createRenderTargets / createShadowMap (renderer.cpp:1240-1453).
@@ -1075,6 +1145,12 @@ private:
 	RestirParams m_params = {};
 	RestirFramePlan m_plan = {};
 	RestirFrameInput m_referenceInput = {};
+	// Orbiting extra lights: accumulated time, two pinned host copies of the moved list.
+	double m_orbitTime = 0.0;
+	float* m_orbitHost[2] = { nullptr, nullptr };
+	size_t m_orbitCapacity[2] = { 0, 0 };
+	cudaEvent_t m_orbitCopied[2] = {};
+	int m_orbitSlot = 0;
 	std::shared_ptr<SceneState> m_scene = std::make_shared<SceneState>();
 	// Set by a batch: the shared shadow atlas and ray queue.
 	float* m_sharedAtlas = nullptr;

@@ -258,7 +258,7 @@ std::vector<uint32_t> randomMaterials(Builder& b, Random& random, int count)
 	return ids;
 }
 
-// 128 emissive panels (256 triangles) of random colour, radiance 4-12.
+// Emissive panels (2 triangles each) of random colour, radiance 4-12.
 void emissivePanels(Builder& b, Random& random, float half, float height, int panels)
 {
 	for (int k = 0; k < panels; ++k)
@@ -314,9 +314,9 @@ Mesh makeCourtyard(uint32_t seed, uint32_t targetTriangles)
 }
 
 // A city block: seeded boxes, spheres of 512 triangles and thin two-sided
-// planes on a ground plane, with 128 emissive panels; about 80% of the
-// triangles in spheres.
-Mesh makeCity(uint32_t seed, uint32_t targetTriangles)
+// planes on a ground plane, with emissive panels (128 by default); about
+// 80% of the triangles in spheres.
+Mesh makeCity(uint32_t seed, uint32_t targetTriangles, int emissivePanelCount)
 {
 	Mesh mesh;
 	Builder b(mesh);
@@ -325,7 +325,7 @@ Mesh makeCity(uint32_t seed, uint32_t targetTriangles)
 	std::vector<uint32_t> mats = randomMaterials(b, random, 128);
 	uint32_t ground = b.material(0.5f, 0.5f, 0.5f, 0.8f);
 	b.quad({ 0.0f, 0.0f, 0.0f }, { half, 0.0f, 0.0f }, { 0.0f, 0.0f, half }, { 0.0f, 1.0f, 0.0f }, ground);
-	emissivePanels(b, random, half * 0.9f, 4.0f, 128);
+	emissivePanels(b, random, half * 0.9f, 4.0f, emissivePanelCount);
 	while (mesh.triangleCount() + 512 <= targetTriangles)
 	{
 		uint32_t m = mats[random.nextU32() % mats.size()];

@@ -262,3 +262,35 @@ def test_small_configuration_sixteen_frames_bit_exact():
     report, oracle_run, _ = run_checked(setup, 256, 256, 16, settings, gi_wavefront=True)
     assert report == {}, report
     assert oracle_run.state.frame_number == 16
+
+
+@pytest.mark.gpu
+def test_orbiting_extra_lights_move_and_hold():
+    """RestirSettings.extra_light_orbit: the extra point lights move on circles
+    about the scene's vertical axis from frame to frame (their height, colour
+    and the emitters stay), and hold still when delta_time is 0."""
+    mesh = rb.Mesh.procedural(rb.SCENE_COURTYARD, 0, 20000)
+    settings = rb.default_settings(mesh)
+    settings.extra_lights = 64
+    settings.extra_light_orbit = 2.0
+    renderer = rb.Renderer(settings)
+    renderer.set_scene(mesh, use_scene_defaults=False)
+    moving = rb.frame_input(mesh, 96, 64, delta_time=0.1)
+    held = rb.frame_input(mesh, 96, 64, delta_time=0.0)
+    lists = []
+    for frame in (moving, moving, held, held):
+        renderer.render(frame)
+        lists.append(renderer.download("lights", np.float32).reshape(-1, 16).copy())
+    center = np.array(mesh.desc.center, np.float32)
+    emitters = int(np.count_nonzero(lists[0][:, 3] == 0.0))
+    a, b = lists[0][emitters:], lists[1][emitters:]
+    assert len(a) == 64 and not np.array_equal(a[:, [0, 2]], b[:, [0, 2]])
+    np.testing.assert_array_equal(a[:, 1], b[:, 1])
+    np.testing.assert_array_equal(a[:, 4:], b[:, 4:])
+    np.testing.assert_allclose(np.hypot(a[:, 0] - center[0], a[:, 2] - center[2]),
+                               np.hypot(b[:, 0] - center[0], b[:, 2] - center[2]), rtol=1e-5)
+    np.testing.assert_array_equal(lists[0][:emitters], lists[1][:emitters])
+    np.testing.assert_array_equal(lists[2], lists[3])
+    hdr = renderer.download("hdr", np.float16)[:96 * 64 * 4].astype(np.float32)
+    assert np.isfinite(hdr).all()
+    renderer.close()

@@ -91,3 +91,15 @@ def test_oracle_only_frames_equal_product_set_up_frames():
     for name in runs[0].buffers:
         np.testing.assert_array_equal(runs[0].host(name), runs[1].host(name), err_msg=name)
     assert np.count_nonzero(runs[0].host("display")) > 0
+
+
+def test_lit_city_has_4096_emissive_triangles():
+    """RESTIR_SCENE_CITY_LIT, the stress configuration's scene: the city with
+    2,048 emissive panels, so the light list holds 4,096 emissive triangles
+    (plus the extra point lights); the oracle's copy of the generator agrees."""
+    from oracle.workload import OracleSetup
+    setup = OracleSetup(rb.SCENE_CITY_LIT, 0, 200_000, extra_lights=1024)
+    assert setup.lights.triangles == 4096 and setup.lights.count == 4096 + 1024
+    product = make_scene(rb.SCENE_CITY_LIT, 0, 200_000, extra_lights=1024)
+    assert product.lights.count == setup.lights.count
+    np.testing.assert_array_equal(setup.lights.data, product.lights.data)
