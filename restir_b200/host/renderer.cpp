@@ -1106,7 +1106,9 @@ private:
 				m_graphExec = nullptr;
 			}
 		}
-		if (!updated && cudaGraphInstantiate(&m_graphExec, graph, 0) != cudaSuccess)
+		// Each kernel node keeps the priority of the stream it was captured on (the main
+		// chain high, the side passes low), as the stream-launched frame runs them.
+		if (!updated && cudaGraphInstantiate(&m_graphExec, graph, cudaGraphInstantiateFlagUseNodePriority) != cudaSuccess)
 		{
 			cudaGraphDestroy(graph);
 			m_graphExec = nullptr;
@@ -1476,7 +1478,9 @@ private:
 				m_graphExec = nullptr;
 			}
 		}
-		if (!updated && cudaGraphInstantiate(&m_graphExec, graph, 0) != cudaSuccess)
+		// Each kernel node keeps the priority of the stream it was captured on (the main
+		// chain high, the side passes low), as the stream-launched frame runs them.
+		if (!updated && cudaGraphInstantiate(&m_graphExec, graph, cudaGraphInstantiateFlagUseNodePriority) != cudaSuccess)
 		{
 			cudaGraphDestroy(graph);
 			m_graphExec = nullptr;
