@@ -217,6 +217,19 @@ int restir_renderer_last_frame(void* renderer, RestirParams* params, RestirFrame
  * "gi.sample", "grid", "reference.mean", ...): pointer and byte size. */
 int restir_renderer_buffer(void* renderer, const char* name, void** pointer, uint64_t* bytes);
 
+/* The per-frame state as a file, so that any frame can be replayed for
+ * debugging (no reference counterpart; the reference's history is per
+ * frame and never saved, renderer.h:87-88): save writes the carried state
+ * (RestirFrameState, the ping-pong indices, the orbit time) and every frame
+ * target (reservoirs, grids, histories, G-buffer, reference mean, TAA and
+ * specular histories) plus the radiance cache's state; load reads such a
+ * file back into a renderer whose targets have the same sizes (render one
+ * frame of that size first) and the same scene and settings. Both wait for
+ * the renderer's streams. RESTIR_ERROR_INVALID_ARGUMENT for a file that does
+ * not match. */
+int restir_renderer_save_state(void* renderer, const char* path);
+int restir_renderer_load_state(void* renderer, const char* path);
+
 /* --- Batches of views (no reference counterpart) ------------------------ */
 
 /* Several views of one scene (each with its own camera and resolution)

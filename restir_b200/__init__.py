@@ -129,6 +129,8 @@ _SIGNATURES = {
     "restir_renderer_last_frame": (C.c_int, [P, C.POINTER(RestirParams), C.POINTER(RestirFramePlan),
                                              C.POINTER(RestirFrameState)]),
     "restir_renderer_buffer": (C.c_int, [P, C.c_char_p, C.POINTER(P), C.POINTER(C.c_uint64)]),
+    "restir_renderer_save_state": (C.c_int, [P, C.c_char_p]),
+    "restir_renderer_load_state": (C.c_int, [P, C.c_char_p]),
     "restir_batch_create": (P, [C.POINTER(RestirSettings), u32]),
     "restir_batch_destroy": (None, [P]),
     "restir_batch_set_scene": (C.c_int, [P, P, C.c_int]),
@@ -455,6 +457,14 @@ class Renderer:
         check(self._lib.restir_renderer_buffer(self.handle, name.encode(), C.byref(pointer), C.byref(nbytes)),
               f"buffer {name}")
         return pointer.value or 0, nbytes.value
+
+    def save_state(self, path) -> None:
+        """The per-frame state (history, reservoirs, grids, ...) to a file (restir_renderer_save_state)."""
+        check(self._lib.restir_renderer_save_state(self.handle, str(path).encode()), "save_state")
+
+    def load_state(self, path) -> None:
+        """Back from a save_state file; the renderer must have rendered a frame of the same size."""
+        check(self._lib.restir_renderer_load_state(self.handle, str(path).encode()), "load_state")
 
     def download(self, name: str, dtype) -> np.ndarray:
         """A copy of one of the renderer's device buffers (after synchronize)."""

@@ -14,8 +14,10 @@
 #include "bvh_build.h"
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -777,11 +779,167 @@ private:
 			&& P.grid_cell_capacity == m_capacity;
 	}
 
+public:
+	// The per-frame state as a file (a debugging aid, no reference
+	// counterpart): the carried state and history indices, then every frame
+	// target (name, size, bytes) and the radiance cache's state when there is
+	// one. Loading needs targets of the same sizes (a frame rendered first).
+	static constexpr char kStateMagic[8] = { 'R', 'S', 'T', 'R', 'S', 'T', '0', '1' };
+
+	struct StateHeader
+	{
+		char magic[8];
+		RestirFrameState state;
+		int32_t historyRead, diRead, taaRead, specularRead, displayTaa;
+		double orbitTime;
+		uint32_t width, height, giWidth, giHeight, faceSize, tableSize, capacity;
+		uint32_t buffers;
+	};
+
+	std::vector<std::pair<std::string, Buffer>> stateBuffers()
+	{
+		std::vector<std::pair<std::string, Buffer>> list(m_targets.begin(), m_targets.end());
+		auto cache = m_scene->buffers.find("cache.state");
+		if (cache != m_scene->buffers.end() && cache->second.pointer != nullptr)
+		{
+			list.emplace_back("cache.state", cache->second);
+		}
+		return list;
+	}
+
+	void synchronizeAll()
+	{
+		cudaStreamSynchronize(m_stream);
+		cudaStreamSynchronize(m_side);
+		cudaStreamSynchronize(m_aside);
+	}
+
+	int saveState(const char* path)
+	{
+		if (path == nullptr || m_targets.empty())
+		{
+			return RESTIR_ERROR_INVALID_ARGUMENT;
+		}
+		synchronizeAll();
+		FILE* file = std::fopen(path, "wb");
+		if (file == nullptr)
+		{
+			return RESTIR_ERROR_INVALID_ARGUMENT;
+		}
+		const auto list = stateBuffers();
+		StateHeader h = {};
+		std::memcpy(h.magic, kStateMagic, sizeof(h.magic));
+		h.state = m_state;
+		h.historyRead = m_historyRead;
+		h.diRead = m_diRead;
+		h.taaRead = m_taaRead;
+		h.specularRead = m_specularRead;
+		h.displayTaa = m_displayTaa ? 1 : 0;
+		h.orbitTime = m_orbitTime;
+		h.width = m_width;
+		h.height = m_height;
+		h.giWidth = m_giWidth;
+		h.giHeight = m_giHeight;
+		h.faceSize = m_faceSize;
+		h.tableSize = m_tableSize;
+		h.capacity = m_capacity;
+		h.buffers = uint32_t(list.size());
+		bool ok = std::fwrite(&h, sizeof(h), 1, file) == 1;
+		std::vector<char> host;
+		for (const auto& entry : list)
+		{
+			const uint32_t length = uint32_t(entry.first.size());
+			const uint64_t bytes = entry.second.bytes;
+			host.resize(bytes);
+			ok = ok && cudaMemcpy(host.data(), entry.second.pointer, bytes, cudaMemcpyDeviceToHost) == cudaSuccess;
+			ok = ok && std::fwrite(&length, sizeof(length), 1, file) == 1
+				&& std::fwrite(entry.first.data(), 1, length, file) == length
+				&& std::fwrite(&bytes, sizeof(bytes), 1, file) == 1
+				&& std::fwrite(host.data(), 1, bytes, file) == bytes;
+		}
+		ok = std::fclose(file) == 0 && ok;
+		return ok ? RESTIR_OK : RESTIR_ERROR_LAUNCH;
+	}
+
+	int loadState(const char* path)
+	{
+		if (path == nullptr || m_targets.empty())
+		{
+			return RESTIR_ERROR_INVALID_ARGUMENT;
+		}
+		synchronizeAll();
+		FILE* file = std::fopen(path, "rb");
+		if (file == nullptr)
+		{
+			return RESTIR_ERROR_INVALID_ARGUMENT;
+		}
+		StateHeader h = {};
+		const auto list = stateBuffers();
+		bool ok = std::fread(&h, sizeof(h), 1, file) == 1 && std::memcmp(h.magic, kStateMagic, sizeof(h.magic)) == 0
+			&& h.width == m_width && h.height == m_height && h.giWidth == m_giWidth && h.giHeight == m_giHeight
+			&& h.faceSize == m_faceSize && h.tableSize == m_tableSize && h.capacity == m_capacity
+			&& h.buffers == uint32_t(list.size());
+		std::vector<char> host;
+		for (uint32_t k = 0; ok && k < h.buffers; ++k)
+		{
+			uint32_t length = 0;
+			uint64_t bytes = 0;
+			std::string name;
+			ok = std::fread(&length, sizeof(length), 1, file) == 1 && length < 256u;
+			if (ok)
+			{
+				name.resize(length);
+				ok = std::fread(&name[0], 1, length, file) == length && std::fread(&bytes, sizeof(bytes), 1, file) == 1;
+			}
+			ok = ok && name == list[k].first && bytes == list[k].second.bytes;
+			if (ok)
+			{
+				host.resize(bytes);
+				ok = std::fread(host.data(), 1, bytes, file) == bytes
+					&& cudaMemcpy(list[k].second.pointer, host.data(), bytes, cudaMemcpyHostToDevice) == cudaSuccess;
+			}
+		}
+		std::fclose(file);
+		if (!ok)
+		{
+			return RESTIR_ERROR_INVALID_ARGUMENT;
+		}
+		m_state = h.state;
+		m_historyRead = h.historyRead;
+		m_diRead = h.diRead;
+		m_taaRead = h.taaRead;
+		m_specularRead = h.specularRead;
+		m_displayTaa = h.displayTaa != 0;
+		m_orbitTime = h.orbitTime;
+		releaseGraph(); // the captured frame reads the history it was recorded with
+		return RESTIR_OK;
+	}
+
+private:
+	// A pass's edges: its CUDA events (timed frames) and an NVTX range around
+	// its launches on the host (the pass groups of the reference's profiler,
+	// renderer.h:45-60), which a timeline profiler shows; without one attached
+	// NVTX does nothing.
+	static const char* passName(int pass)
+	{
+		static const char* const kNames[RESTIR_PASS_COUNT] = { "shadow", "gbuffer", "di_temporal", "di_spatial", "grid",
+			"gi_temporal", "gi_spatial", "denoise", "composite", "reference", "cache", "display", "specular" };
+		return pass >= 0 && pass < RESTIR_PASS_COUNT ? kNames[pass] : "pass";
+	}
+
 	void mark(int pass, int edge, bool events)
 	{
+		if (edge == 0)
+		{
+			nvtxRangePushA(passName(pass));
+		}
 		if (events)
 		{
 			cudaEventRecord(m_events[m_slot][pass][edge], m_stream);
+		}
+		if (edge == 1)
+		{
+			nvtxRangePop();
 		}
 	}
 
@@ -847,7 +1005,9 @@ private:
 			{
 				cudaEventRecord(m_events[m_slot][pass][0], m_aside);
 			}
+			nvtxRangePushA(passName(pass));
 			status |= body(static_cast<void*>(m_aside));
+			nvtxRangePop();
 			m_passRan[m_slot][pass] = true;
 			if (events)
 			{
@@ -1648,6 +1808,16 @@ extern "C" int restir_renderer_last_frame(void* renderer, RestirParams* params, 
 	}
 	static_cast<Renderer*>(renderer)->lastFrame(params, plan, state);
 	return RESTIR_OK;
+}
+
+extern "C" int restir_renderer_save_state(void* renderer, const char* path)
+{
+	return renderer == nullptr ? RESTIR_ERROR_INVALID_ARGUMENT : static_cast<Renderer*>(renderer)->saveState(path);
+}
+
+extern "C" int restir_renderer_load_state(void* renderer, const char* path)
+{
+	return renderer == nullptr ? RESTIR_ERROR_INVALID_ARGUMENT : static_cast<Renderer*>(renderer)->loadState(path);
 }
 
 extern "C" int restir_renderer_buffer(void* renderer, const char* name, void** pointer, uint64_t* bytes)

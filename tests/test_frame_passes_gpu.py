@@ -294,3 +294,44 @@ def test_orbiting_extra_lights_move_and_hold():
     hdr = renderer.download("hdr", np.float16)[:96 * 64 * 4].astype(np.float32)
     assert np.isfinite(hdr).all()
     renderer.close()
+
+
+@pytest.mark.gpu
+def test_saved_state_replays_the_following_frames(tmp_path):
+    """restir_renderer_save_state / load_state: a second renderer loaded with
+    the state saved after frame 3 renders frames 4 and 5 bit for bit as the
+    first renderer does (history, reservoirs, grids, TAA and specular
+    histories, frame number)."""
+    mesh = rb.Mesh.procedural(rb.SCENE_COURTYARD, 1, 20000)
+    frame = rb.frame_input(mesh, 160, 96)
+
+    def make():
+        settings = rb.default_settings(mesh)
+        settings.grid_mode = rb.GRID_DETERMINISTIC
+        settings.extra_lights = 16
+        r = rb.Renderer(settings)
+        r.set_scene(mesh, use_scene_defaults=False)
+        return r
+
+    first = make()
+    for _ in range(3):
+        first.render(frame)
+    path = tmp_path / "frame3.state"
+    first.save_state(path)
+    for _ in range(2):
+        first.render(frame)
+    second = make()
+    second.render(frame)  # targets of the same size
+    second.load_state(path)
+    for _ in range(2):
+        second.render(frame)
+    for name in ("display.hdr", "hdr", "display", "gi.sample0", "gi.sample1", "grid0", "grid1"):
+        np.testing.assert_array_equal(first.download(name, np.uint8), second.download(name, np.uint8), err_msg=name)
+    assert first.last_frame()[2].frame_number == second.last_frame()[2].frame_number == 5
+    # A file for targets of another size is refused.
+    third = make()
+    third.render(rb.frame_input(mesh, 64, 64))
+    with pytest.raises(RuntimeError):
+        third.load_state(path)
+    for r in (first, second, third):
+        r.close()
