@@ -411,7 +411,8 @@ uint64_t restir_struct_size(const char* name);
  * step cap, bit 1 a hash grid probe sequence was exhausted, bit 2 a ray
  * queue was full (rays past its capacity are not traced), bit 3 a
  * tensor-core step of the radiance cache failed (a bounded wait gave up or a
- * shared-memory tile was misaligned; that launch's results are invalid). */
+ * shared-memory tile was misaligned; that launch's results are invalid), bit
+ * 4 an index out of range (bounds-checked builds, RESTIR_CHECKS=1, only). */
 int restir_status(uint32_t* flags);
 
 /* Work counters: waits for the device, returns the counts gathered since the

@@ -57,6 +57,7 @@ def _run(command: list[str]) -> None:
 
 
 FAST_LIBRARY = PACKAGE / "librestir_gpu_fast.so"
+CHECKED_LIBRARY = PACKAGE / "librestir_gpu_checked.so"
 
 
 def build(verbose: bool = False, defines: list[str] | None = None, library: Path = LIBRARY,
@@ -99,7 +100,10 @@ def build(verbose: bool = False, defines: list[str] | None = None, library: Path
 
 
 if __name__ == "__main__":
-    if "--contract" in sys.argv:
+    if "--checks" in sys.argv:
+        print(build(verbose="-v" in sys.argv, defines=["RESTIR_CHECKS=1"], library=CHECKED_LIBRARY,
+                    objects_dir=BUILD.parent / "_build_checked"))
+    elif "--contract" in sys.argv:
         print(build(verbose="-v" in sys.argv, library=FAST_LIBRARY, objects_dir=BUILD.parent / "_build_contract",
                     contract=True))
     else:

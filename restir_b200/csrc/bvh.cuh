@@ -22,10 +22,15 @@ struct BvhView
 	const float4* rows = nullptr;
 	int nodeCount = 0;
 	int triangleOffset = 0;
+	int rowCount = 0;   // nodes x 2 + triangles x 4 (checked builds test indices against it)
 
 	__device__ __forceinline__ bool available() const { return nodeCount > 0; }
 	__device__ __forceinline__ V4 row(int i) const
 	{
+		if (!checkedIndex(uint32_t(i), uint32_t(rowCount)))
+		{
+			return { 0.0f, 0.0f, 0.0f, 0.0f };
+		}
 		float4 q = __ldg(rows + i);
 		return { q.x, q.y, q.z, q.w };
 	}
@@ -46,6 +51,7 @@ __host__ __device__ inline BvhView makeBvhView(const RestirScene* s)
 		b.rows = reinterpret_cast<const float4*>(s->bvh);
 		b.nodeCount = int(s->node_count);
 		b.triangleOffset = int(s->triangle_offset);
+		b.rowCount = int(s->triangle_offset + 4u * s->triangle_count);
 	}
 	return b;
 }

@@ -270,6 +270,30 @@ __device__ __forceinline__ void countWork(int kind, uint32_t nodes, uint32_t tri
 	}
 }
 
+// Bounds-checked builds (RESTIR_CHECKS=1: python -m restir_b200.build
+// --checks, librestir_gpu_checked.so), the stand-in for a memory checker:
+// every BVH row and light-list row index is tested before the load; one out
+// of range raises status bit 4 and reads zeros instead, so a broken input is
+// reported, not followed outside its buffer. Off in the product build.
+#ifndef RESTIR_CHECKS
+#define RESTIR_CHECKS 0
+#endif
+
+__device__ __forceinline__ bool checkedIndex(uint32_t index, uint32_t count)
+{
+#if RESTIR_CHECKS
+	if (index >= count)
+	{
+		raiseStatus(16u);
+		return false;
+	}
+#else
+	(void)index;
+	(void)count;
+#endif
+	return true;
+}
+
 // A traversal stopped short (the 2,048-visit cap, bvh.sh:23, or a full
 // traversal stack): status bit 0, and one ray counted while counting is on.
 __device__ __forceinline__ void reportTruncatedRay()

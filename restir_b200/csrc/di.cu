@@ -92,6 +92,10 @@ struct DiPass
 	__device__ __forceinline__ int lightCount() const { return P.di_light_count; }
 	__device__ __forceinline__ V4 lightData(int light, int row) const
 	{
+		if (!checkedIndex(uint32_t(light), uint32_t(lightCount())))
+		{
+			return { 0.0f, 0.0f, 0.0f, 0.0f };
+		}
 		float4 q = __ldg(lights + light * 4 + row);
 		return { q.x, q.y, q.z, q.w };
 	}
