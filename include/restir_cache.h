@@ -16,8 +16,11 @@
  *     Multiresolution Hash Encoding", 2022): RESTIR_CACHE_LEVELS levels of
  *     RESTIR_CACHE_FEATURES half-precision features, trilinear, level l at
  *     resolution floor(n_min * b^l), b = (n_max / n_min)^(1 / (levels - 1)),
- *     dense indexing where the level's (res + 1)^3 corners fit the table,
- *     else (x * 1 ^ y * 2654435761 ^ z * 805459861) mod table size;
+ *     corners stored in 2x2x2 bricks of 8 consecutive entries (one 32-byte
+ *     sector: a cell's corners touch 3.4 sectors on average, not up to 8),
+ *     brick (x / 2, y / 2, z / 2) numbered densely where the level's bricks
+ *     fit the table (8 * ceil((res + 1) / 2)^3 <= entries), else hashed as
+ *     (bx * 1 ^ by * 2654435761 ^ bz * 805459861) mod (entries / 8);
  *   - 64 inputs: the 32 encoded features, direction (3), normal (3),
  *     roughness, albedo (3), a constant 1, zeros; rounded to bfloat16;
  *   - 4 hidden layers of 64 (ReLU), 3 outputs (linear) padded to 16, no

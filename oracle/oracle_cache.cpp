@@ -6,7 +6,8 @@
  * algorithms the header names: the multiresolution hash encoding (Mueller,
  * Evans, Schied, Keller 2022, section 3: per-level trilinear interpolation of
  * hashed corner features, hash = XOR of the coordinates times the primes
- * 1, 2654435761, 805459861, dense indexing where a level fits), a ReLU MLP
+ * 1, 2654435761, 805459861, dense indexing where a level fits; here applied
+ * to 2x2x2 bricks of corners stored together), a ReLU MLP
  * without biases, the relative L2 loss of neural radiance caching (Mueller,
  * Rousselle, Novak, Keller 2021, section 5: (y - t)^2 / (sg(y)^2 + 0.01)),
  * its gradients by backpropagation, and Adam (Kingma and Ba 2015,
@@ -58,7 +59,7 @@ void corners(const RestirCacheLayout& l, int level, const float unit[3], Corners
 		cell[a] = std::min(int(std::floor(g)), resolution - 1);
 		frac[a] = g - float(cell[a]);
 	}
-	const uint32_t side = uint32_t(resolution + 1);
+	const uint32_t bricks = uint32_t(resolution + 2) / 2u;
 	for (int d = 0; d < 8; ++d)
 	{
 		const int bx = d & 1, by = (d >> 1) & 1, bz = d >> 2;
@@ -68,8 +69,12 @@ void corners(const RestirCacheLayout& l, int level, const float unit[3], Corners
 		const float wz = bz ? frac[2] : 1.0f - frac[2];
 		const float wxy = wx * wy;
 		out.weight[d] = wxy * wz;
-		out.index[d] = l.level_dense[level] ? x + y * side + z * side * side
-			: ((x * 1u) ^ (y * 2654435761u) ^ (z * 805459861u)) & (l.entries - 1u);
+		// 2x2x2 bricks of 8 consecutive entries (restir_cache.h).
+		const uint32_t local = (x % 2u) + 2u * (y % 2u) + 4u * (z % 2u);
+		const uint32_t cx = x / 2u, cy = y / 2u, cz = z / 2u;
+		const uint32_t brick = l.level_dense[level] ? cx + cy * bricks + cz * bricks * bricks
+			: ((cx * 1u) ^ (cy * 2654435761u) ^ (cz * 805459861u)) % (l.entries / 8u);
+		out.index[d] = brick * 8u + local;
 	}
 }
 

@@ -83,6 +83,23 @@ __device__ __forceinline__ float unitCoordinate(float p, float lo, float hi)
 	return fminf(fmaxf((p - lo) / (hi - lo), 0.0f), 1.0f);
 }
 
+// The table slot of corner (x, y, z): corners are stored in 2x2x2 bricks of
+// 8 consecutive entries (32 bytes of half features, one L2 sector), so a
+// cell's 8 corners fall in 1, 2, 4 or 8 sectors (3.4 on average) instead of
+// up to 8. A dense level numbers the bricks x + y * b + z * b^2; a hashed
+// level hashes the brick coordinates (XOR of the coordinates times 1,
+// 2654435761, 805459861, as Mueller et al. 2022 hash corners) onto the
+// table's entries / 8 bricks.
+__device__ __forceinline__ uint32_t brickIndex(bool dense, uint32_t x, uint32_t y, uint32_t z, uint32_t bricks,
+	uint32_t entries)
+{
+	const uint32_t local = (x & 1u) | ((y & 1u) << 1) | ((z & 1u) << 2);
+	const uint32_t bx = x >> 1, by = y >> 1, bz = z >> 1;
+	const uint32_t brick = dense ? bx + by * bricks + bz * bricks * bricks
+		: ((bx * 1u) ^ (by * 2654435761u) ^ (bz * 805459861u)) & ((entries >> 3) - 1u);
+	return brick * 8u + local;
+}
+
 __device__ __forceinline__ void levelCorners(const CacheView& c, int level, const float unit[3], LevelCorners& out)
 {
 	const float scale = c.levelScale[level];
@@ -96,7 +113,7 @@ __device__ __forceinline__ void levelCorners(const CacheView& c, int level, cons
 		frac[a] = g - float(cell[a]);
 	}
 	const bool dense = (c.denseLevels >> level) & 1u;
-	const uint32_t side = uint32_t(resolution + 1);
+	const uint32_t bricks = uint32_t(resolution + 2) >> 1;  // bricks across a dense level
 	for (int d = 0; d < 8; ++d)
 	{
 		const uint32_t x = uint32_t(cell[0] + (d & 1));
@@ -106,8 +123,7 @@ __device__ __forceinline__ void levelCorners(const CacheView& c, int level, cons
 		const float wy = ((d >> 1) & 1) ? frac[1] : 1.0f - frac[1];
 		const float wz = (d >> 2) ? frac[2] : 1.0f - frac[2];
 		out.weight[d] = wx * wy * wz;
-		out.index[d] = dense ? x + y * side + z * side * side
-			: ((x * 1u) ^ (y * 2654435761u) ^ (z * 805459861u)) & (c.entries - 1u);
+		out.index[d] = brickIndex(dense, x, y, z, bricks, c.entries);
 	}
 }
 

@@ -90,8 +90,9 @@ extern "C" int restir_cache_layout(const RestirCacheConfig* cfg, RestirCacheLayo
 	{
 		const double resolution = std::floor(double(cfg->n_min) * std::pow(growth, double(level)) + 1e-9);
 		l.level_scale[level] = float(resolution);
-		const double corners = (resolution + 1.0) * (resolution + 1.0) * (resolution + 1.0);
-		l.level_dense[level] = corners <= double(l.entries) ? 1u : 0u;
+		// Dense when the level's 2x2x2 bricks of corners, 8 entries each, fit the table.
+		const double bricks = std::floor((resolution + 2.0) / 2.0);
+		l.level_dense[level] = 8.0 * bricks * bricks * bricks <= double(l.entries) ? 1u : 0u;
 	}
 	*layout = l;
 	return RESTIR_OK;

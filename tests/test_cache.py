@@ -29,7 +29,7 @@ def test_layout():
     assert all(float(s).is_integer() for s in scales)
     entries = 1 << 12
     for s, dense in zip(scales, layout.level_dense):
-        assert bool(dense) == ((s + 1) ** 3 <= entries)
+        assert bool(dense) == (8 * ((int(s) + 2) // 2) ** 3 <= entries)
     assert layout.table_half - layout.table == 16 * entries * 2 * 4
     bad = rb.cache_config(table_log2=30)
     assert rb.load().restir_cache_layout(C.byref(bad), C.byref(abi.RestirCacheLayout())) == rb.ERROR_INVALID_ARGUMENT
