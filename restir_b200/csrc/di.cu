@@ -66,18 +66,11 @@ __device__ __forceinline__ void evaluateBrdf(V3 n, V3 v, V3 l, V3 albedo, float 
 	diffuse = (v3s(1.0f) - fresnel) * (1.0f - metallic) * albedo / kPi * normalLight;
 }
 
-// The light list's CDF (row 2 .w of each light, lights.h) staged in shared
-// memory by the DI temporal kernel when it has at most this many lights: the
-// candidates' binary searches (selectLight) then read shared memory instead
-// of 64-byte-strided list rows. Same values, same search: same lights.
-constexpr int kSharedCdfLights = 2048;
-
 struct DiPass
 {
 	const RestirParams& P;
 	BvhView bvh;
 	const float4* lights;
-	const float* sharedCdf = nullptr; // the CDF in shared memory, or null
 	const uint8_t* albedoTex;
 	const uint8_t* normalTex;
 	const uint8_t* shadingTex;
@@ -128,8 +121,7 @@ struct DiPass
 		for (int step = 0; step < 24 && low < high; ++step)
 		{
 			int middle = (low + high) >> 1;
-			const float cdf = sharedCdf != nullptr ? sharedCdf[middle] : __ldg(&lights[middle * 4 + 2].w);
-			if (cdf < random)
+			if (__ldg(&lights[middle * 4 + 2].w) < random)
 			{
 				low = middle + 1;
 			}
@@ -234,21 +226,9 @@ __device__ __forceinline__ DiPass makeDiPass(const RestirParams& P, const BvhVie
 __global__ void __launch_bounds__(128, RESTIR_DI_TEMPORAL_MIN_BLOCKS) diTemporalKernel(const RestirParams P, BvhView bvh, const float* lights, RestirGBuffer gb,
 	RestirDiReservoirs previous, RestirDiReservoirs out)
 {
-	__shared__ float cdf[kSharedCdfLights];
-	const bool cdfShared = P.di_light_count <= kSharedCdfLights;
-	if (cdfShared)
-	{
-		const float4* rows = reinterpret_cast<const float4*>(lights);
-		for (int k = int(threadIdx.x); k < P.di_light_count; k += int(blockDim.x))
-		{
-			cdf[k] = __ldg(&rows[k * 4 + 2].w);
-		}
-	}
-	__syncthreads();
 	const int px = int(blockIdx.x * 16 + threadIdx.x % 16);
 	const int py = int(blockIdx.y * 8 + threadIdx.x / 16);
 	DiPass d = makeDiPass(P, bvh, lights, gb);
-	d.sharedCdf = cdfShared ? cdf : nullptr;
 	if (px >= d.W || py >= d.H)
 	{
 		return;
