@@ -12,8 +12,9 @@
 // backward pass and accumulates the weight gradients of all its tiles in
 // TMEM (dW = dZ^T H, with K = the 128 rows of a tile), then writes one row
 // of per-block partial sums; a reduction kernel sums the rows in a fixed
-// order, so training is deterministic apart from the hash-table gradient,
-// which is scattered with atomics.
+// order. The hash-table gradient is scattered with atomics onto 64-bit
+// fixed-point sums, whose integer addition does not depend on the order the
+// atomics land in, so a training step is deterministic.
 #include "common.cuh"
 #include "umma.cuh"
 
@@ -134,10 +135,106 @@ __device__ __forceinline__ void unitPosition(const CacheView& c, const float4& q
 	unit[2] = unitCoordinate(q0.z, c.boundsMin[2], c.boundsMax[2]);
 }
 
-// Two floats as a pair of bfloat16 (lo in the low half).
+// Two floats as a pair of bfloat16 (lo in the low half), one cvt
+// instruction. The conversion rounds to nearest even as restir_numeric.h's
+// rn_float_to_bf16 does, so the bits are the same for every non-NaN input.
 __device__ __forceinline__ uint32_t packBf16(float lo, float hi)
 {
-	return uint32_t(rn_float_to_bf16(lo)) | (uint32_t(rn_float_to_bf16(hi)) << 16);
+	uint32_t pair;
+	asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(pair) : "f"(hi), "f"(lo));
+	return pair;
+}
+
+// The two halves of a pair of FP16 features as floats (exact conversions).
+__device__ __forceinline__ void unpackHalf2(uint32_t pair, float& lo, float& hi)
+{
+	asm("{\n\t.reg .b16 l, h;\n\tmov.b32 {l, h}, %2;\n\tcvt.f32.f16 %0, l;\n\tcvt.f32.f16 %1, h;\n\t}"
+		: "=f"(lo), "=f"(hi) : "r"(pair));
+}
+
+// A float as FP16, rounded to nearest even (rn_float_to_half's bits for
+// every non-NaN input).
+__device__ __forceinline__ uint16_t toHalf(float f)
+{
+	uint16_t h;
+	asm("cvt.rn.f16.f32 %0, %1;" : "=h"(h) : "f"(f));
+	return h;
+}
+
+__device__ __forceinline__ uint4 choose(bool p, const uint4& a, const uint4& b)
+{
+	return make_uint4(p ? a.x : b.x, p ? a.y : b.y, p ? a.z : b.z, p ? a.w : b.w);
+}
+
+// Entry (b0 + 2 b1) of a 16-byte half brick (4 entries: local x + 2 y).
+__device__ __forceinline__ uint32_t pickEntry(const uint4& h, bool b0, bool b1)
+{
+	const uint32_t lo = b0 ? h.y : h.x;
+	const uint32_t hi = b0 ? h.w : h.z;
+	return b1 ? hi : lo;
+}
+
+// The feature pairs of a cell's 8 corners on one level, each brick half
+// read once. A brick's two 16-byte halves are its z = 0 and z = 1 planes
+// (locals 0-3 and 4-7). Along an axis where the cell's coordinate is even
+// both corners lie in one brick; where it is odd they lie in neighbouring
+// bricks. So the corners of plane ez (z = cell z + ez) sit in at most 2 x 2
+// half bricks, columns (dx, dy) with dx <= odd x, dy <= odd y; these are
+// loaded (the others are predicated off), 2 to 8 loads of 16 bytes and
+// 3.4 sectors on average instead of 8 loads of 4 bytes in as many sectors,
+// and each corner picks its entry. The values are the ones levelCorners'
+// indices address.
+__device__ __forceinline__ void levelPairs(const CacheView& c, int level, const int cell[3], uint32_t pair[8])
+{
+	const bool dense = (c.denseLevels >> level) & 1u;
+	const uint32_t bricks = uint32_t(int(c.levelScale[level]) + 2) >> 1;
+	const uint32_t mask = (c.entries >> 3) - 1u;
+	const uint32_t bx = uint32_t(cell[0]) >> 1, by = uint32_t(cell[1]) >> 1, bz = uint32_t(cell[2]) >> 1;
+	const bool ox = cell[0] & 1, oy = cell[1] & 1, oz = cell[2] & 1;
+	// brickIndex's terms per axis, for brick offsets 0 and 1.
+	uint32_t tx[2], ty[2], tz[2];
+	for (uint32_t k = 0; k < 2; ++k)
+	{
+		tx[k] = dense ? bx + k : (bx + k) * 1u;
+		ty[k] = dense ? (by + k) * bricks : (by + k) * 2654435761u;
+		tz[k] = dense ? (bz + k) * bricks * bricks : (bz + k) * 805459861u;
+	}
+	const uint4* table = reinterpret_cast<const uint4*>(c.tableHalf) + size_t(level) * (c.entries >> 2);
+#pragma unroll
+	for (int ez = 0; ez < 2; ++ez)
+	{
+		// The plane's brick along z and its half: z = cell z + ez.
+		const uint32_t zTerm = tz[oz && ez];
+		const uint32_t half = uint32_t(oz != bool(ez));
+		uint4 h[2][2];
+#pragma unroll
+		for (int dy = 0; dy < 2; ++dy)
+		{
+#pragma unroll
+			for (int dx = 0; dx < 2; ++dx)
+			{
+				h[dy][dx] = make_uint4(0u, 0u, 0u, 0u);
+				if ((dx == 0 || ox) && (dy == 0 || oy))
+				{
+					const uint32_t brick = dense ? tx[dx] + ty[dy] + zTerm : (tx[dx] ^ ty[dy] ^ zTerm) & mask;
+					h[dy][dx] = __ldg(table + size_t(brick) * 2u + half);
+				}
+			}
+		}
+		// Corner (ex, ey): column (ox & ex, oy & ey), entry ((ox ^ ex), (oy ^ ey)).
+#pragma unroll
+		for (int ey = 0; ey < 2; ++ey)
+		{
+#pragma unroll
+			for (int ex = 0; ex < 2; ++ex)
+			{
+				const bool cx = ox && ex, cy = oy && ey;
+				const uint4 lo = choose(cx, h[0][1], h[0][0]);
+				const uint4 hi = choose(cx, h[1][1], h[1][0]);
+				pair[ex + 2 * ey + 4 * ez] = pickEntry(choose(cy, hi, lo), ox != bool(ex), oy != bool(ey));
+			}
+		}
+	}
 }
 
 // The 64 network inputs of one query as bfloat16, 8 per 16-byte chunk. The
@@ -152,21 +249,34 @@ __device__ inline void queryFeatures(const CacheView& c, const float4* query, ui
 #pragma unroll
 	for (int level = 0; level < RESTIR_CACHE_LEVELS; ++level)
 	{
-		LevelCorners corners;
-		levelCorners(c, level, unit, corners);
-		const uint32_t* row = reinterpret_cast<const uint32_t*>(c.tableHalf) + size_t(level) * c.entries;
+		const float scale = c.levelScale[level];
+		const int resolution = int(scale);
+		int cell[3];
+		float frac[3];
+		for (int a = 0; a < 3; ++a)
+		{
+			const float g = unit[a] * scale;
+			cell[a] = min(int(floorf(g)), resolution - 1);
+			frac[a] = g - float(cell[a]);
+		}
 		uint32_t pair[8];
-#pragma unroll
+		levelPairs(c, level, cell, pair);
+		LevelCorners corners;
 		for (int d = 0; d < 8; ++d)
 		{
-			pair[d] = __ldg(row + corners.index[d]);
+			const float wx = (d & 1) ? frac[0] : 1.0f - frac[0];
+			const float wy = ((d >> 1) & 1) ? frac[1] : 1.0f - frac[1];
+			const float wz = (d >> 2) ? frac[2] : 1.0f - frac[2];
+			corners.weight[d] = wx * wy * wz;
 		}
 		float f0 = 0.0f, f1 = 0.0f;
 #pragma unroll
 		for (int d = 0; d < 8; ++d)
 		{
-			f0 = f0 + corners.weight[d] * rn_half_to_float(uint16_t(pair[d] & 0xffffu));
-			f1 = f1 + corners.weight[d] * rn_half_to_float(uint16_t(pair[d] >> 16));
+			float h0, h1;
+			unpackHalf2(pair[d], h0, h1);
+			f0 = f0 + corners.weight[d] * h0;
+			f1 = f1 + corners.weight[d] * h1;
 		}
 		packed[level] = packBf16(f0, f1);
 	}
@@ -223,26 +333,46 @@ __device__ __forceinline__ void loadWeights(uint8_t* smem, const uint16_t* weigh
 // ReLU of 16 accumulator columns into 2 chunks of bfloat16.
 __device__ __forceinline__ void reluChunks(const float* v, uint4* chunk)
 {
-	uint16_t h[16];
-	for (int i = 0; i < 16; ++i)
+	uint32_t h[8];
+	for (int i = 0; i < 8; ++i)
 	{
-		h[i] = rn_float_to_bf16(fmaxf(v[i], 0.0f));
+		h[i] = packBf16(fmaxf(v[2 * i], 0.0f), fmaxf(v[2 * i + 1], 0.0f));
 	}
-	for (int k = 0; k < 2; ++k)
-	{
-		chunk[k] = make_uint4(uint32_t(h[8 * k]) | (uint32_t(h[8 * k + 1]) << 16), uint32_t(h[8 * k + 2]) | (uint32_t(h[8 * k + 3]) << 16),
-			uint32_t(h[8 * k + 4]) | (uint32_t(h[8 * k + 5]) << 16), uint32_t(h[8 * k + 6]) | (uint32_t(h[8 * k + 7]) << 16));
-	}
+	chunk[0] = make_uint4(h[0], h[1], h[2], h[3]);
+	chunk[1] = make_uint4(h[4], h[5], h[6], h[7]);
 }
 
 // The CTA's tensor-core context: its TMEM columns, its mbarrier and phase.
 struct TensorContext
 {
-	uint32_t tmem;
-	uint32_t barrier;
-	uint32_t phase;
-	bool ok;
+	uint32_t tmem = 0;
+	uint32_t barrier = 0;
+	uint32_t phase = 0;
+	bool ok = true;
+	int group = 0;  // the tile group of 128 threads that owns the context (named barrier 1 + group)
 };
+
+// The 128 threads of tile group g meet at named barrier 1 + g (barrier 0 is
+// __syncthreads'), so the groups of a block run their tiles independently.
+__device__ __forceinline__ void groupSync(int group)
+{
+	asm volatile("bar.sync %0, 128;" ::"r"(group + 1) : "memory");
+}
+
+// The group's barrier as a vote: true if `p` holds in all its 128 threads.
+__device__ __forceinline__ bool groupAll(int group, bool p)
+{
+	uint32_t all;
+	asm volatile(
+		"{\n\t.reg .pred p, q;\n\t"
+		"setp.ne.u32 p, %1, 0;\n\t"
+		"bar.red.and.pred q, %2, 128, p;\n\t"
+		"selp.u32 %0, 1, 0, q;\n\t}\n"
+		: "=r"(all)
+		: "r"(p ? 1u : 0u), "r"(group + 1)
+		: "memory");
+	return all != 0u;
+}
 
 // Every thread waits for the barrier's current phase, at most `polls` polls;
 // a wait that gives up raises status bit 3 and marks the context failed (the
@@ -251,10 +381,10 @@ __device__ __forceinline__ void awaitBarrier(TensorContext& t, uint32_t polls)
 {
 	bool done = umma::barrierWait(t.barrier, t.phase, polls);
 	t.phase ^= 1u;
-	done = __syncthreads_and(done) != 0;
+	done = groupAll(t.group, done);
 	if (!done)
 	{
-		if (threadIdx.x == 0)
+		if ((threadIdx.x & (kTile - 1)) == 0)
 		{
 			raiseStatus(kStatusTensor);
 		}
@@ -263,10 +393,12 @@ __device__ __forceinline__ void awaitBarrier(TensorContext& t, uint32_t polls)
 	umma::fenceAfterSync();
 }
 
-// Commit by the issuing thread, then every thread waits for the MMAs.
+// Commit by the issuing thread (the group's first), then every thread of the
+// group waits for the MMAs. A commit tracks the MMAs its own thread issued,
+// so the groups of a block complete independently.
 __device__ __forceinline__ void completeMmas(TensorContext& t)
 {
-	if (threadIdx.x == 0)
+	if ((threadIdx.x & (kTile - 1)) == 0)
 	{
 		umma::commit(t.barrier);
 	}
@@ -283,6 +415,7 @@ __global__ void __launch_bounds__(128) waitCheckKernel(uint32_t polls, uint32_t*
 	t.phase = 0;
 	t.ok = true;
 	t.tmem = 0;
+	t.group = 0;
 	if (threadIdx.x == 0)
 	{
 		umma::barrierInit(t.barrier, 1);
@@ -322,6 +455,15 @@ __device__ __forceinline__ void handOff()
 	umma::fenceAfterSync();
 }
 
+// The same within one tile group.
+__device__ __forceinline__ void groupHandOff(int group)
+{
+	umma::fenceSharedForAsync();
+	umma::fenceBeforeSync();
+	groupSync(group);
+	umma::fenceAfterSync();
+}
+
 // D (128 x n) = A (128 x 64, K-major tile) * W^T for one layer with n outputs.
 __device__ __forceinline__ void issueLayer(uint32_t tmemD, const uint8_t* a, const uint8_t* w, int n)
 {
@@ -336,35 +478,51 @@ __device__ __forceinline__ void issueLayer(uint32_t tmemD, const uint8_t* a, con
 
 // --- forward ----------------------------------------------------------------------------
 
-constexpr int kForwardSmem = kWeightBytes + kTileBytes + 64;
+// A forward block runs kGroups tile groups of 128 threads (4 warps each),
+// which share one copy of the weights in shared memory and each own an
+// activation tile, an mbarrier and 64 TMEM columns: the weights are paid
+// once per block, so more tiles are in flight per SM, and each group's
+// gathers overlap the other groups' MMA chains. Named barriers keep the
+// groups independent. Blocks per SM: 4 of 1 group (128 registers a thread),
+// 3 of 2 (80), 2 of 4 (64). On 2,073,600 random queries 4 groups measured
+// 1.170 ms against 1.196 (2) and 1.200 (1): the encoding's gathers bound
+// all three, so the renderer uses 4.
+constexpr int kForwardGroups = 4;
 
-template<int kMode>  // 0: half4 cache values, 1: 16 raw floats, 2: the 64 inputs
-__global__ void __launch_bounds__(kTile, 4) forwardKernel(CacheView c, const float4* __restrict__ queries, uint32_t n,
-	void* __restrict__ output)
+template<int kGroups>
+struct ForwardShape
+{
+	static constexpr int threads = kTile * kGroups;
+	static constexpr int blocksPerSm = kGroups == 1 ? 4 : (kGroups == 2 ? 3 : 2);
+	static constexpr int smem = kWeightBytes + kGroups * kTileBytes + 64;
+	static constexpr uint32_t columns = 64u * uint32_t(kGroups);
+};
+
+template<int kMode, int kGroups>  // kMode 0: half4 cache values, 1: 16 raw floats, 2: the 64 inputs
+__global__ void __launch_bounds__(ForwardShape<kGroups>::threads, ForwardShape<kGroups>::blocksPerSm)
+	forwardKernel(CacheView c, const float4* __restrict__ queries, uint32_t n, void* __restrict__ output)
 {
 	extern __shared__ __align__(1024) uint8_t smem[];
-	uint8_t* weights = smem;
-	uint8_t* act = smem + kWeightBytes;
-	uint64_t* barrier = reinterpret_cast<uint64_t*>(smem + kWeightBytes + kTileBytes);
-	uint32_t* slot = reinterpret_cast<uint32_t*>(smem + kWeightBytes + kTileBytes + 8);
 	const int tid = int(threadIdx.x);
 	const int warp = tid >> 5;
+	const int group = tid / kTile;
+	const int r = tid % kTile;  // the thread's row of its group's tile and its TMEM lane
+	uint8_t* weights = smem;
+	uint8_t* act = smem + kWeightBytes + group * kTileBytes;
+	uint64_t* barriers = reinterpret_cast<uint64_t*>(smem + kWeightBytes + kGroups * kTileBytes);
+	uint32_t* slot = reinterpret_cast<uint32_t*>(barriers + kGroups);
 	const uint32_t tiles = (n + kTile - 1) / kTile;
 
 	if (kMode == 2)
 	{
-		for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x)
+		for (uint32_t row = blockIdx.x * blockDim.x + uint32_t(tid); row < n; row += gridDim.x * blockDim.x)
 		{
-			const uint32_t row = tile * kTile + uint32_t(tid);
-			if (row < n)
+			uint4 chunk[8];
+			queryFeatures(c, queries + size_t(row) * 4, chunk);
+			uint4* out = static_cast<uint4*>(output) + size_t(row) * 8;
+			for (int k = 0; k < 8; ++k)
 			{
-				uint4 chunk[8];
-				queryFeatures(c, queries + size_t(row) * 4, chunk);
-				uint4* out = static_cast<uint4*>(output) + size_t(row) * 8;
-				for (int k = 0; k < 8; ++k)
-				{
-					out[k] = chunk[k];
-				}
+				out[k] = chunk[k];
 			}
 		}
 		return;
@@ -375,27 +533,30 @@ __global__ void __launch_bounds__(kTile, 4) forwardKernel(CacheView c, const flo
 		return;
 	}
 	loadWeights(weights, c.weightsBf16);
-	TensorContext t;
-	t.barrier = umma::smemAddress(barrier);
-	t.phase = 0;
-	t.ok = true;
-	if (tid == 0)
+	if (tid < kGroups)
 	{
-		umma::barrierInit(t.barrier, 1);
+		umma::barrierInit(umma::smemAddress(barriers + tid), 1);
 	}
 	if (warp == 0)
 	{
-		umma::tmemAllocate(umma::smemAddress(slot), 64);
+		umma::tmemAllocate(umma::smemAddress(slot), ForwardShape<kGroups>::columns);
 	}
 	umma::fenceBeforeSync();
 	__syncthreads();
 	umma::fenceAfterSync();
-	t.tmem = *slot;
-	const uint32_t laneBase = uint32_t(warp * 32) << 16;
+	const uint32_t tmemBase = *slot;
+	TensorContext t;
+	t.tmem = tmemBase + 64u * uint32_t(group);
+	t.barrier = umma::smemAddress(barriers + group);
+	t.phase = 0;
+	t.ok = true;
+	t.group = group;
+	// A warp reads the TMEM lanes of its quarter of the group: 32 * (warp % 4).
+	const uint32_t laneBase = uint32_t((warp & 3) * 32) << 16;
 
-	for (uint32_t tile = blockIdx.x; tile < tiles && t.ok; tile += gridDim.x)
+	for (uint32_t tile = blockIdx.x * kGroups + uint32_t(group); tile < tiles && t.ok; tile += gridDim.x * kGroups)
 	{
-		const uint32_t row = tile * kTile + uint32_t(tid);
+		const uint32_t row = tile * kTile + uint32_t(r);
 		uint4 chunk[8];
 		if (row < n)
 		{
@@ -408,12 +569,12 @@ __global__ void __launch_bounds__(kTile, 4) forwardKernel(CacheView c, const flo
 				chunk[k] = make_uint4(0u, 0u, 0u, 0u);
 			}
 		}
-		storeRow(act, tid, chunk);
+		storeRow(act, r, chunk);
 		for (int layer = 0; layer < 5 && t.ok; ++layer)
 		{
-			handOff();
+			groupHandOff(group);
 			const int width = layer < 4 ? 64 : 16;
-			if (tid == 0)
+			if (r == 0)
 			{
 				issueLayer(t.tmem, act, weights + layer * kWeightLayerBytes, width);
 			}
@@ -430,8 +591,8 @@ __global__ void __launch_bounds__(kTile, 4) forwardKernel(CacheView c, const flo
 					umma::tmemLoad16(t.tmem + laneBase + uint32_t(16 * q), v);
 					uint4 relu[2];
 					reluChunks(v, relu);
-					*reinterpret_cast<uint4*>(act + umma::coreOffset(uint32_t(tid), uint32_t(16 * q), 64u)) = relu[0];
-					*reinterpret_cast<uint4*>(act + umma::coreOffset(uint32_t(tid), uint32_t(16 * q + 8), 64u)) = relu[1];
+					*reinterpret_cast<uint4*>(act + umma::coreOffset(uint32_t(r), uint32_t(16 * q), 64u)) = relu[0];
+					*reinterpret_cast<uint4*>(act + umma::coreOffset(uint32_t(r), uint32_t(16 * q + 8), 64u)) = relu[1];
 				}
 			}
 			else
@@ -443,10 +604,10 @@ __global__ void __launch_bounds__(kTile, 4) forwardKernel(CacheView c, const flo
 					if (kMode == 0)
 					{
 						ushort4 h;
-						h.x = rn_float_to_half(fmaxf(v[0], 0.0f));
-						h.y = rn_float_to_half(fmaxf(v[1], 0.0f));
-						h.z = rn_float_to_half(fmaxf(v[2], 0.0f));
-						h.w = rn_float_to_half(queries[size_t(row) * 4 + 1].w > 0.5f ? 1.0f : 0.0f);
+						h.x = toHalf(fmaxf(v[0], 0.0f));
+						h.y = toHalf(fmaxf(v[1], 0.0f));
+						h.z = toHalf(fmaxf(v[2], 0.0f));
+						h.w = toHalf(queries[size_t(row) * 4 + 1].w > 0.5f ? 1.0f : 0.0f);
 						static_cast<ushort4*>(output)[row] = h;
 					}
 					else
@@ -466,7 +627,7 @@ __global__ void __launch_bounds__(kTile, 4) forwardKernel(CacheView c, const flo
 	if (warp == 0)
 	{
 		umma::fenceAfterSync();
-		umma::tmemFree(t.tmem, 64);
+		umma::tmemFree(tmemBase, ForwardShape<kGroups>::columns);
 	}
 }
 
@@ -1044,6 +1205,23 @@ bool prepare(const RestirCacheConfig* cfg, const void* state, RestirCacheLayout&
 		&& restir_cache_layout(cfg, &l) == RESTIR_OK;
 }
 
+template<int kMode, int kGroups>
+void launchForwardShape(const CacheView& view, const float4* queries, uint32_t n, void* output, void* stream)
+{
+	using Shape = ForwardShape<kGroups>;
+	static bool configured = false;
+	if (!configured)
+	{
+		cudaFuncSetAttribute(forwardKernel<kMode, kGroups>, cudaFuncAttributeMaxDynamicSharedMemorySize, Shape::smem);
+		configured = true;
+	}
+	const uint32_t tiles = (n + kTile - 1) / kTile;
+	// At most the blocks that fit on the SMs at once (shared memory, registers
+	// and TMEM: blocksPerSm x columns <= 512); each loops over tiles.
+	const uint32_t blocks = min((tiles + kGroups - 1) / kGroups, uint32_t(smCount() * Shape::blocksPerSm));
+	forwardKernel<kMode, kGroups><<<blocks, Shape::threads, Shape::smem, asStream(stream)>>>(view, queries, n, output);
+}
+
 template<int kMode>
 int launchForward(const RestirCacheConfig* cfg, const void* state, const float* queries, uint32_t n, void* output,
 	void* stream)
@@ -1057,17 +1235,8 @@ int launchForward(const RestirCacheConfig* cfg, const void* state, const float* 
 	{
 		return RESTIR_OK;
 	}
-	static bool configured = false;
-	if (!configured)
-	{
-		cudaFuncSetAttribute(forwardKernel<kMode>, cudaFuncAttributeMaxDynamicSharedMemorySize, kForwardSmem);
-		configured = true;
-	}
-	const uint32_t tiles = (n + kTile - 1) / kTile;
-	// Up to 4 blocks of 64 TMEM columns per SM (shared memory allows 4).
-	const uint32_t blocks = min(tiles, uint32_t(smCount() * 4));
-	forwardKernel<kMode><<<blocks, kTile, kForwardSmem, asStream(stream)>>>(makeView(*cfg, l, state),
-		reinterpret_cast<const float4*>(queries), n, output);
+	launchForwardShape<kMode, kForwardGroups>(makeView(*cfg, l, state), reinterpret_cast<const float4*>(queries), n, output,
+		stream);
 	return launchStatus();
 }
 
