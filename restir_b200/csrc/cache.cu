@@ -174,16 +174,31 @@ __device__ __forceinline__ uint32_t pickEntry(const uint4& h, bool b0, bool b1)
 	return b1 ? hi : lo;
 }
 
-// The feature pairs of a cell's 8 corners on one level, each brick half
-// read once. A brick's two 16-byte halves are its z = 0 and z = 1 planes
-// (locals 0-3 and 4-7). Along an axis where the cell's coordinate is even
-// both corners lie in one brick; where it is odd they lie in neighbouring
-// bricks. So the corners of plane ez (z = cell z + ez) sit in at most 2 x 2
-// half bricks, columns (dx, dy) with dx <= odd x, dy <= odd y; these are
-// loaded (the others are predicated off), 2 to 8 loads of 16 bytes and
-// 3.4 sectors on average instead of 8 loads of 4 bytes in as many sectors,
-// and each corner picks its entry. The values are the ones levelCorners'
-// indices address.
+// A whole brick (8 entries, 32 bytes: one L2 sector) in one 256-bit load;
+// a brick starts on a 32-byte boundary (the table is 256-byte aligned and a
+// level is a whole number of bricks).
+struct Brick
+{
+	uint4 lo;  // the z = 0 plane: locals 0-3
+	uint4 hi;  // the z = 1 plane: locals 4-7
+};
+
+__device__ __forceinline__ Brick loadBrick(const uint4* p)
+{
+	Brick b;
+	asm("ld.global.nc.v8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+		: "=r"(b.lo.x), "=r"(b.lo.y), "=r"(b.lo.z), "=r"(b.lo.w), "=r"(b.hi.x), "=r"(b.hi.y), "=r"(b.hi.z), "=r"(b.hi.w)
+		: "l"(p));
+	return b;
+}
+
+// The feature pairs of a cell's 8 corners on one level, each brick read
+// once. Along an axis where the cell's coordinate is even both corners lie
+// in one brick; where it is odd they lie in neighbouring bricks. So the
+// corners sit in (1 + odd x)(1 + odd y)(1 + odd z) bricks, 3.4 on average:
+// those are loaded whole (the others are predicated off) instead of 8
+// 4-byte loads in as many sectors, and each corner picks its entry. The
+// values are the ones levelCorners' indices address.
 __device__ __forceinline__ void levelPairs(const CacheView& c, int level, const int cell[3], uint32_t pair[8])
 {
 	const bool dense = (c.denseLevels >> level) & 1u;
@@ -200,28 +215,37 @@ __device__ __forceinline__ void levelPairs(const CacheView& c, int level, const 
 		tz[k] = dense ? (bz + k) * bricks * bricks : (bz + k) * 805459861u;
 	}
 	const uint4* table = reinterpret_cast<const uint4*>(c.tableHalf) + size_t(level) * (c.entries >> 2);
+	// plane[ez][dy][dx]: the 4 entries (local x + 2 y) of corner plane z = cell z + ez
+	// in brick column (dx, dy): with z even both planes are the brick's; with z
+	// odd plane 0 is the upper half of brick z and plane 1 the lower half of brick z + 1.
+	uint4 plane[2][2][2];
+#pragma unroll
+	for (int dy = 0; dy < 2; ++dy)
+	{
+#pragma unroll
+		for (int dx = 0; dx < 2; ++dx)
+		{
+			Brick b0 = { make_uint4(0u, 0u, 0u, 0u), make_uint4(0u, 0u, 0u, 0u) };
+			Brick b1 = b0;
+			if ((dx == 0 || ox) && (dy == 0 || oy))
+			{
+				const uint32_t column = dense ? tx[dx] + ty[dy] : tx[dx] ^ ty[dy];
+				const uint32_t brick0 = dense ? column + tz[0] : (column ^ tz[0]) & mask;
+				b0 = loadBrick(table + size_t(brick0) * 2u);
+				if (oz)
+				{
+					const uint32_t brick1 = dense ? column + tz[1] : (column ^ tz[1]) & mask;
+					b1 = loadBrick(table + size_t(brick1) * 2u);
+				}
+			}
+			plane[0][dy][dx] = choose(oz, b0.hi, b0.lo);
+			plane[1][dy][dx] = choose(oz, b1.lo, b0.hi);
+		}
+	}
+	// Corner (ex, ey, ez): column (ox & ex, oy & ey), entry ((ox ^ ex), (oy ^ ey)).
 #pragma unroll
 	for (int ez = 0; ez < 2; ++ez)
 	{
-		// The plane's brick along z and its half: z = cell z + ez.
-		const uint32_t zTerm = tz[oz && ez];
-		const uint32_t half = uint32_t(oz != bool(ez));
-		uint4 h[2][2];
-#pragma unroll
-		for (int dy = 0; dy < 2; ++dy)
-		{
-#pragma unroll
-			for (int dx = 0; dx < 2; ++dx)
-			{
-				h[dy][dx] = make_uint4(0u, 0u, 0u, 0u);
-				if ((dx == 0 || ox) && (dy == 0 || oy))
-				{
-					const uint32_t brick = dense ? tx[dx] + ty[dy] + zTerm : (tx[dx] ^ ty[dy] ^ zTerm) & mask;
-					h[dy][dx] = __ldg(table + size_t(brick) * 2u + half);
-				}
-			}
-		}
-		// Corner (ex, ey): column (ox & ex, oy & ey), entry ((ox ^ ex), (oy ^ ey)).
 #pragma unroll
 		for (int ey = 0; ey < 2; ++ey)
 		{
@@ -229,13 +253,14 @@ __device__ __forceinline__ void levelPairs(const CacheView& c, int level, const 
 			for (int ex = 0; ex < 2; ++ex)
 			{
 				const bool cx = ox && ex, cy = oy && ey;
-				const uint4 lo = choose(cx, h[0][1], h[0][0]);
-				const uint4 hi = choose(cx, h[1][1], h[1][0]);
+				const uint4 lo = choose(cx, plane[ez][0][1], plane[ez][0][0]);
+				const uint4 hi = choose(cx, plane[ez][1][1], plane[ez][1][0]);
 				pair[ex + 2 * ey + 4 * ez] = pickEntry(choose(cy, hi, lo), ox != bool(ex), oy != bool(ey));
 			}
 		}
 	}
 }
+
 
 // The 64 network inputs of one query as bfloat16, 8 per 16-byte chunk. The
 // levels are unrolled so that the gathers of all levels can be in flight
@@ -484,10 +509,10 @@ __device__ __forceinline__ void issueLayer(uint32_t tmemD, const uint8_t* a, con
 // once per block, so more tiles are in flight per SM, and each group's
 // gathers overlap the other groups' MMA chains. Named barriers keep the
 // groups independent. Blocks per SM: 4 of 1 group (128 registers a thread),
-// 3 of 2 (80), 2 of 4 (64). On 2,073,600 random queries 4 groups measured
-// 1.170 ms against 1.196 (2) and 1.200 (1): the encoding's gathers bound
-// all three, so the renderer uses 4.
-constexpr int kForwardGroups = 4;
+// 3 of 2 (80), 2 of 4 (64). With the encoding's whole-brick loads, on
+// 2,073,600 random queries: 1 group 0.934 ms, 2 groups 0.947, 4 groups 1.132
+// (at 64 registers the 16 levels' brick loads spill); the renderer uses 1.
+constexpr int kForwardGroups = 1;
 
 template<int kGroups>
 struct ForwardShape
