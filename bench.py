@@ -887,8 +887,9 @@ def own_arm(args, rank: int, world: int) -> None:
                                  "peak": l2_gather_gbs, "frac": fetched_gbs / l2_gather_gbs, "unit": "GB/s",
                                  "peak_source": "restir_gather_probe: random 32-byte gathers from the scene's BVH "
                                                 "nodes (L2-resident), measured in this run"},
-                     "limiter": "instruction issue and SIMT efficiency of divergent traversal (ncu: 9.5 of 32 "
-                                "lanes active per instruction in the queue tracer), not DRAM bandwidth"},
+                     "limiter": "instruction issue and SIMT efficiency of divergent traversal (ncu: 9.3 of 32 "
+                                "lanes active per instruction in the queue tracer, 66% of issue slots busy), "
+                                "not DRAM bandwidth"},
         "cpu_baseline": baseline,
         "clocks": clocks,
     }
