@@ -91,6 +91,59 @@ __device__ __forceinline__ V4 f4(float4 q)
 	return { q.x, q.y, q.z, q.w };
 }
 
+// The end of the temporal pass: the boiling filter against the group's mean
+// estimate (summed as compute.sh's shared-memory tree), then the reservoir's
+// store. Every lane of the warp calls it.
+__device__ __forceinline__ void boilAndStore(const RestirParams& P, const GiPass& g, const GiBindings& b, int lane, bool inside,
+	bool working, int px, int py, V3 position, V3 normal, V3 albedo, const GiReservoir& canonical, float canonicalWeight,
+	V2 previousUv, const PairwiseMis& mis, float combinedWeight)
+{
+	const bool historyValid = P.history_valid > 0.5f;
+	const float estimate = working ? mis.combined.target * combinedWeight : 0.0f;
+	float sumEstimate = estimate;
+	float sumWorking = working ? 1.0f : 0.0f;
+	for (int stride = 16; stride > 0; stride >>= 1)
+	{
+		float e = __shfl_down_sync(0xffffffffu, sumEstimate, stride);
+		float c = __shfl_down_sync(0xffffffffu, sumWorking, stride);
+		if (lane < stride)
+		{
+			sumEstimate += e;
+			sumWorking += c;
+		}
+	}
+	sumEstimate = __shfl_sync(0xffffffffu, sumEstimate, 0);
+	sumWorking = __shfl_sync(0xffffffffu, sumWorking, 0);
+	const float tileMean = sumEstimate / fmaxf(sumWorking, 1.0f);
+	if (working && P.boiling_filter > 0.0f && combinedWeight > 0.0f)
+	{
+		float reference = canonical.target * canonicalWeight;
+		V3 historyColor;
+		if (historyValid && g.historyIrradiance(previousUv, position, normal, historyColor))
+		{
+			reference = fmaxf(reference, luminance(historyColor * albedo));
+		}
+		else
+		{
+			reference = fmaxf(reference, tileMean);
+		}
+		float limit = P.boiling_filter * reference;
+		if (estimate > limit)
+		{
+			combinedWeight *= limit / estimate;
+		}
+	}
+	if (inside)
+	{
+		const int i = py * g.w + px;
+		b.outSample[i] = working ? make_float4(mis.combined.position.x, mis.combined.position.y, mis.combined.position.z,
+			mis.totalCount) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+		b.outReceiver[i] = working ? make_float4(position.x, position.y, position.z, combinedWeight)
+			: make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+		b.outNormal[i] = working ? make_float4(normal.x, normal.y, normal.z, mis.combined.id) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+	}
+}
+
 // cs_restir_temporal.sc:192-296 after the fresh candidates: temporal reuse
 // with pairwise MIS, the boiling filter over the warp's 4x8 group, the
 // reservoir stores. Every lane of the warp must call it (the group sum).
@@ -150,51 +203,8 @@ __device__ __forceinline__ void temporalReuseAndStore(const RestirParams& P, con
 		}
 		combinedWeight = g.finishPairwiseMis(mis, position, normal, canonical, canonicalWeight, nextRandom(rng));
 	}
-
-	// Boiling filter: the group's mean estimate, summed as compute.sh's tree.
-	const float estimate = working ? mis.combined.target * combinedWeight : 0.0f;
-	float sumEstimate = estimate;
-	float sumWorking = working ? 1.0f : 0.0f;
-	for (int stride = 16; stride > 0; stride >>= 1)
-	{
-		float e = __shfl_down_sync(0xffffffffu, sumEstimate, stride);
-		float c = __shfl_down_sync(0xffffffffu, sumWorking, stride);
-		if (lane < stride)
-		{
-			sumEstimate += e;
-			sumWorking += c;
-		}
-	}
-	sumEstimate = __shfl_sync(0xffffffffu, sumEstimate, 0);
-	sumWorking = __shfl_sync(0xffffffffu, sumWorking, 0);
-	const float tileMean = sumEstimate / fmaxf(sumWorking, 1.0f);
-	if (working && P.boiling_filter > 0.0f && combinedWeight > 0.0f)
-	{
-		float reference = canonical.target * canonicalWeight;
-		V3 historyColor;
-		if (historyValid && g.historyIrradiance(previousUv, position, normal, historyColor))
-		{
-			reference = fmaxf(reference, luminance(historyColor * albedo));
-		}
-		else
-		{
-			reference = fmaxf(reference, tileMean);
-		}
-		float limit = P.boiling_filter * reference;
-		if (estimate > limit)
-		{
-			combinedWeight *= limit / estimate;
-		}
-	}
-	if (inside)
-	{
-		const int i = py * g.w + px;
-		b.outSample[i] = working ? make_float4(mis.combined.position.x, mis.combined.position.y, mis.combined.position.z,
-			mis.totalCount) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-		b.outReceiver[i] = working ? make_float4(position.x, position.y, position.z, combinedWeight)
-			: make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-		b.outNormal[i] = working ? make_float4(normal.x, normal.y, normal.z, mis.combined.id) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-	}
+	boilAndStore(P, g, b, lane, inside, working, px, py, position, normal, albedo, canonical, canonicalWeight, previousUv, mis,
+		combinedWeight);
 }
 
 __global__ void __launch_bounds__(kGiThreads, RESTIR_GI_TEMPORAL_MIN_BLOCKS) giTemporalKernel(const RestirParams P, BvhView bvh,
@@ -558,61 +568,177 @@ __global__ void __launch_bounds__(kGiThreads, RESTIR_GI_TEMPORAL_MIN_BLOCKS) giT
 	uint32_t rng = pcg(uint32_t(giPixelCoord.x) + pcg(uint32_t(giPixelCoord.y) + pcg(uint32_t(P.frame_index))));
 	const int pixel = py * g.w + px;
 
-	GiReservoir canonical = emptyReservoir();
-	for (int sampleIndex = 0; sampleIndex < P.initial_candidates; ++sampleIndex)
+	// The candidates, the temporal reuse (temporalReuseAndStore) and the
+	// combination as one loop with one call site each for the sample
+	// evaluation and the visibility test (the kernel is bound by instruction
+	// fetch): steps 0..C-1 shade the candidates, steps C..C+T-1 take the
+	// temporal neighbours and step C+T combines, the last two for working
+	// pixels only. The random draws and every operation are the
+	// straight-line form's, in its order.
+	const int candidates = P.initial_candidates;
+	const int taps = P.temporal_taps;
+	const int last = working ? candidates + taps : candidates - 1;
+	const bool historyValid = P.history_valid > 0.5f;
+	V2 previousUv = v2(0.0f, 0.0f);
+	const V4 clipPrevious = mul(P.prev_view_proj, v4(position, 1.0f));
+	if (clipPrevious.w > 0.0001f)
 	{
-		float random0 = nextRandom(rng);
-		float random1 = nextRandom(rng);
-		float randomSelect = nextRandom(rng);
-		V3 direction = GiPass::cosineHemisphere(normal, random0, random1);
-		canonical.count += 1.0f;
-		V3 hitPosition = v3s(0.0f);
-		float hitId = 0.0f;
-		bool hit = false;
-		if (inside)
+		previousUv = clipToUv(P, clipPrevious);
+	}
+	const float radius = g.reuseRadius(position);
+	GiReservoir canonical = emptyReservoir();
+	float canonicalWeight = 0.0f;
+	PairwiseMis mis;
+	float combinedWeight = 0.0f;
+	bool misStarted = false;
+#pragma unroll 1
+	for (int step = 0; step <= last; ++step)
+	{
+		if (step >= candidates && !misStarted)
 		{
-			const int r = pixel * records.candidates + sampleIndex;
-			const float4 screen = records.screenHit[r];
-			hit = screen.w > 0.5f;
-			hitPosition = v3(screen.x, screen.y, screen.z);
-			const int slot = records.slot[r];
-			// -3: the BVH was wanted but there is none (traceBvh returns -1 at once).
-			if (slot >= 0 || slot == -3)
+			canonicalWeight = canonical.target > 0.000001f ? canonical.weightSum / (canonical.count * canonical.target) : 0.0f;
+			mis = g.beginPairwiseMis(position, normal, canonical, canonical.count, taps);
+			misStarted = true;
+		}
+		// What this step evaluates and tests.
+		bool evaluate = false;
+		V3 samplePosition = v3s(0.0f);
+		float sampleId = 0.0f;
+		int cacheSlot = -1;
+		V3 direction = v3s(0.0f);
+		float randomSelect = 0.0f;
+		NeighbourReservoir neighbour;
+		float neighbourGeometry = 0.0f;
+		bool test = false;
+		V3 from = position, fromNormal = normal, to = v3s(0.0f);
+		float toId = 0.0f;
+		if (step < candidates)
+		{
+			const int sampleIndex = step;
+			float random0 = nextRandom(rng);
+			float random1 = nextRandom(rng);
+			randomSelect = nextRandom(rng);
+			direction = GiPass::cosineHemisphere(normal, random0, random1);
+			canonical.count += 1.0f;
+			bool hit = false;
+			if (inside)
 			{
-				int triangle = -1;
-				float t = 0.0f;
-				if (slot >= 0)
+				const int r = pixel * records.candidates + sampleIndex;
+				const float4 screen = records.screenHit[r];
+				hit = screen.w > 0.5f;
+				samplePosition = v3(screen.x, screen.y, screen.z);
+				const int slot = records.slot[r];
+				// -3: the BVH was wanted but there is none (traceBvh returns -1 at once).
+				if (slot >= 0 || slot == -3)
 				{
-					triangle = queue.hitTriangle[slot];
-					t = queue.hitDistance[slot];
-				}
-				if (triangle >= 0)
-				{
-					hit = true;
-					hitPosition = rayOrigin + direction * t;
-					hitId = g.encodeSampleId(triangle, direction);
-				}
-				else if (skyEnabled(P))
-				{
-					hit = true;
-					hitPosition = direction;
-					hitId = kSkySampleId;
+					int triangle = -1;
+					float t = 0.0f;
+					if (slot >= 0)
+					{
+						triangle = queue.hitTriangle[slot];
+						t = queue.hitDistance[slot];
+					}
+					if (triangle >= 0)
+					{
+						hit = true;
+						samplePosition = rayOrigin + direction * t;
+						sampleId = g.encodeSampleId(triangle, direction);
+					}
+					else if (skyEnabled(P))
+					{
+						hit = true;
+						samplePosition = direction;
+						sampleId = kSkySampleId;
+					}
 				}
 			}
+			evaluate = hit;
+			cacheSlot = g.cache != nullptr ? pixel * records.candidates + sampleIndex : -1;
+		}
+		else if (step < candidates + taps)
+		{
+			const int tapIndex = step - candidates;
+			float random0 = nextRandom(rng);
+			float random1 = nextRandom(rng);
+			float random2 = nextRandom(rng);
+			randomSelect = nextRandom(rng);
+			V2 historyUv = v2(-1.0f, -1.0f);
+			if (historyValid)
+			{
+				if (g.grid.worldSpace)
+				{
+					uint32_t entry = gridPickEntry(g.grid, position, normal, random0, random1, random2);
+					if (entry != kGridInvalid)
+					{
+						historyUv = g.giPixelUv(entry);
+					}
+				}
+				else if (tapIndex == 0 && clipPrevious.w > 0.0001f)
+				{
+					historyUv = previousUv;
+				}
+			}
+			bool accepted = false;
+			if (isOnScreen(historyUv))
+			{
+				int i = g.gi(historyUv);
+				accepted = g.acceptNeighbour(f4(__ldg(b.historySample + i)), f4(__ldg(b.historyReceiver + i)),
+					f4(__ldg(b.historyNormal + i)), position, normal, radius, neighbour);
+				neighbour.cacheSlot = g.cache != nullptr ? g.cacheNeighbourBase + i : -1;
+			}
+			if (!accepted)
+			{
+				GiPass::skipNeighbour(mis);
+				continue;
+			}
+			test = g.neighbourBegin(mis, neighbour, neighbourGeometry);
+			from = neighbour.receiverPosition;
+			fromNormal = neighbour.receiverNormal;
+			to = mis.canonicalPosition;
+			toId = mis.canonicalId;
+		}
+		else
+		{
+			test = g.finishBegin(mis, canonical, canonicalWeight, nextRandom(rng), combinedWeight);
+			to = mis.combined.position;
+			toId = mis.combined.id;
+		}
+		const bool occluded = test && !g.isVisible(from, fromNormal, to, toId);
+		if (step == candidates + taps)
+		{
+			if (occluded)
+			{
+				combinedWeight = 0.0f;
+			}
+			break;
+		}
+		if (step >= candidates)
+		{
+			g.neighbourShare(mis, neighbour, neighbourGeometry, occluded);
+			evaluate = neighbour.weight > 0.0f;
+			samplePosition = neighbour.samplePosition;
+			sampleId = neighbour.sampleId;
+			cacheSlot = neighbour.cacheSlot;
 		}
 		V3 contribution = v3s(0.0f);
-		V3 hitNormal = v3s(0.0f);
-		bool evaluated = false;
-		if (hit)
+		V3 sampleNormal = step < candidates ? v3s(0.0f) : v3(0.0f, 0.0f, 1.0f);
+		bool valid = false;
+		if (evaluate)
 		{
-			const int cacheSlot = g.cache != nullptr ? pixel * records.candidates + sampleIndex : -1;
-			evaluated = g.evaluateSample(position, normal, albedo, hitPosition, hitId, contribution, hitNormal, cacheSlot);
+			valid = g.evaluateSample(position, normal, albedo, samplePosition, sampleId, contribution, sampleNormal, cacheSlot);
 		}
-		if (evaluated)
+		if (step >= candidates)
 		{
+			g.neighbourShift(mis, position, normal, neighbour, valid, contribution, sampleNormal, randomSelect);
+		}
+		else if (valid)
+		{
+			// The candidate's source density and its update (cs_restir_temporal.sc).
+			const V3 hitPosition = samplePosition;
+			const V3 hitNormal = sampleNormal;
 			float target = luminance(contribution);
 			float sourcePdf = dot(normal, direction) / kPi;
-			if (!isSkySample(hitId))
+			if (!isSkySample(sampleId))
 			{
 				V3 fromReceiver = hitPosition - position;
 				V3 fromOrigin = hitPosition - rayOrigin;
@@ -626,11 +752,17 @@ __global__ void __launch_bounds__(kGiThreads, RESTIR_GI_TEMPORAL_MIN_BLOCKS) giT
 			}
 			if (target > 0.0f && sourcePdf > 0.0001f)
 			{
-				updateReservoir(canonical, contribution, hitPosition, hitNormal, hitId, target, target / sourcePdf, randomSelect);
+				updateReservoir(canonical, contribution, hitPosition, hitNormal, sampleId, target, target / sourcePdf, randomSelect);
 			}
 		}
 	}
-	temporalReuseAndStore(P, g, b, lane, inside, working, px, py, position, normal, albedo, canonical, rng);
+	if (!misStarted)
+	{
+		canonicalWeight = canonical.target > 0.000001f ? canonical.weightSum / (canonical.count * canonical.target) : 0.0f;
+		mis = g.beginPairwiseMis(position, normal, canonical, canonical.count, taps);
+	}
+	boilAndStore(P, g, b, lane, inside, working, px, py, position, normal, albedo, canonical, canonicalWeight, previousUv, mis,
+		combinedWeight);
 }
 
 // --- indirect specular (fs_specular.sc) --------------------------------------------------

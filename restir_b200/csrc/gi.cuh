@@ -653,40 +653,57 @@ struct GiPass
 		mis.canonicalShare += mis.pairCanonical;
 	}
 
-	__device__ inline void addNeighbour(PairwiseMis& mis, V3 p, V3 n, V3 albedo, const NeighbourReservoir& nb, float random) const
+	// addNeighbour and finishPairwiseMis in parts around their visibility test
+	// and sample evaluation, so that a kernel can run all of its reuse's tests
+	// and evaluations at one call site each (its code then fits the
+	// instruction cache); the arithmetic is the same either way.
+	//
+	// Neighbour, part 1: the count, and the canonical sample's geometry term
+	// at the neighbour; true when that term needs the visibility test from the
+	// neighbour's receiver to the canonical sample.
+	__device__ __forceinline__ bool neighbourBegin(PairwiseMis& mis, const NeighbourReservoir& nb, float& neighbourGeometry) const
 	{
-		float neighbourCount = nb.count;
-		float pairWeight = neighbourCount + mis.pairCanonical;
-		mis.totalCount += neighbourCount;
+		mis.totalCount += nb.count;
+		neighbourGeometry = 0.0f;
+		if (!mis.hasCanonical)
+		{
+			return false;
+		}
+		neighbourGeometry = geometryTerm(nb.receiverPosition, nb.receiverNormal, mis.canonicalPosition, mis.canonicalNormal,
+			mis.canonicalId);
+		return neighbourGeometry > 0.0f;
+	}
+
+	// Neighbour, part 2: the canonical sample's pairwise share, given the test.
+	__device__ __forceinline__ void neighbourShare(PairwiseMis& mis, const NeighbourReservoir& nb, float neighbourGeometry,
+		bool occluded) const
+	{
 		if (mis.hasCanonical)
 		{
-			float neighbourGeometry = geometryTerm(nb.receiverPosition, nb.receiverNormal, mis.canonicalPosition,
-				mis.canonicalNormal, mis.canonicalId);
-			if (neighbourGeometry > 0.0f)
+			if (occluded)
 			{
-				if (!isVisible(nb.receiverPosition, nb.receiverNormal, mis.canonicalPosition, mis.canonicalId))
-				{
-					neighbourGeometry = 0.0f;
-				}
+				neighbourGeometry = 0.0f;
 			}
+			float pairWeight = nb.count + mis.pairCanonical;
 			float canonicalDensity = mis.pairCanonical * mis.canonicalGeometry;
-			float denominator = neighbourCount * neighbourGeometry + canonicalDensity;
+			float denominator = nb.count * neighbourGeometry + canonicalDensity;
 			mis.canonicalShare += denominator > 0.0f ? pairWeight * canonicalDensity / denominator : pairWeight;
 		}
-		V3 contribution = v3s(0.0f);
-		V3 sampleNormal = v3(0.0f, 0.0f, 1.0f);
-		bool shifted = false;
-		if (nb.weight > 0.0f)
-		{
-			shifted = evaluateSample(p, n, albedo, nb.samplePosition, nb.sampleId, contribution, sampleNormal, nb.cacheSlot);
-		}
+	}
+
+	// Neighbour, part 3: its sample shifted to this pixel, from the sample's
+	// evaluation here (evaluated only when nb.weight > 0).
+	__device__ __forceinline__ void neighbourShift(PairwiseMis& mis, V3 p, V3 n, const NeighbourReservoir& nb, bool shifted,
+		V3 contribution, V3 sampleNormal, float random) const
+	{
 		if (shifted)
 		{
+			float pairWeight = nb.count + mis.pairCanonical;
 			float target = luminance(contribution);
 			float jacobian = reconnectionJacobian(p, nb.receiverPosition, nb.samplePosition, sampleNormal, nb.sampleId);
 			float hereGeometry = geometryTerm(p, n, nb.samplePosition, sampleNormal, nb.sampleId);
 			float thereGeometry = geometryTerm(nb.receiverPosition, nb.receiverNormal, nb.samplePosition, sampleNormal, nb.sampleId);
-			float neighbourDensity = neighbourCount * thereGeometry;
+			float neighbourDensity = nb.count * thereGeometry;
 			float denominator = neighbourDensity + mis.pairCanonical * hereGeometry;
 			float misWeight = denominator > 0.0f ? pairWeight * neighbourDensity / denominator : 0.0f;
 			float weight = misWeight * target * nb.weight * jacobian;
@@ -698,8 +715,30 @@ struct GiPass
 		}
 	}
 
-	__device__ inline float finishPairwiseMis(PairwiseMis& mis, V3 p, V3 n, const GiReservoir& canonical, float canonicalWeight,
-		float random) const
+	__device__ inline void addNeighbour(PairwiseMis& mis, V3 p, V3 n, V3 albedo, const NeighbourReservoir& nb, float random) const
+	{
+		float neighbourGeometry;
+		bool occluded = false;
+		if (neighbourBegin(mis, nb, neighbourGeometry))
+		{
+			occluded = !isVisible(nb.receiverPosition, nb.receiverNormal, mis.canonicalPosition, mis.canonicalId);
+		}
+		neighbourShare(mis, nb, neighbourGeometry, occluded);
+		V3 contribution = v3s(0.0f);
+		V3 sampleNormal = v3(0.0f, 0.0f, 1.0f);
+		bool shifted = false;
+		if (nb.weight > 0.0f)
+		{
+			shifted = evaluateSample(p, n, albedo, nb.samplePosition, nb.sampleId, contribution, sampleNormal, nb.cacheSlot);
+		}
+		neighbourShift(mis, p, n, nb, shifted, contribution, sampleNormal, random);
+	}
+
+	// The combination, part 1: the canonical sample's update and the combined
+	// weight; true when a chosen neighbour's sample needs the visibility test
+	// from this pixel (part 2: a failed test zeroes the weight).
+	__device__ __forceinline__ bool finishBegin(PairwiseMis& mis, const GiReservoir& canonical, float canonicalWeight, float random,
+		float& combinedWeight) const
 	{
 		if (mis.hasCanonical)
 		{
@@ -710,10 +749,17 @@ struct GiPass
 				mis.neighbourSelected = false;
 			}
 		}
-		float combinedWeight = mis.combined.target > 0.000001f
+		combinedWeight = mis.combined.target > 0.000001f
 			? mis.combined.weightSum / (mis.totalCount * mis.combined.target)
 			: 0.0f;
-		if (combinedWeight > 0.0f && mis.neighbourSelected)
+		return combinedWeight > 0.0f && mis.neighbourSelected;
+	}
+
+	__device__ inline float finishPairwiseMis(PairwiseMis& mis, V3 p, V3 n, const GiReservoir& canonical, float canonicalWeight,
+		float random) const
+	{
+		float combinedWeight;
+		if (finishBegin(mis, canonical, canonicalWeight, random, combinedWeight))
 		{
 			if (!isVisible(p, n, mis.combined.position, mis.combined.id))
 			{
