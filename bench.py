@@ -370,7 +370,7 @@ def pareto(args) -> None:
     """--pareto: the metric's comparison at equal error. Both forms (plain and
     radiance cache) over PARETO_VARIANTS on the 1920x1080 city view, each pair
     from a fresh renderer (fresh history and, for the cache form, a fresh
-    cache): the 64-frame FP64 reference with the default settings, then the
+    cache): the 1,024-frame FP64 reference with the default settings, then the
     variant's settings, warm-up (CACHE_TRAIN_FRAMES of training for the cache
     form), device ms/frame over `steps` frames (CUDA events) and the mean
     relMSE over ERROR_FRAMES frames; then, per form, the cheapest setting
