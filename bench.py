@@ -50,7 +50,7 @@ REFERENCE_FRAMES = 1024
 ERROR_FRAMES = 120         # frames the relMSE and bias are averaged over
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per frame of the GI temporal pass's
 # three kernels on this workload, one launch each, captured from the current build.
-DOMINANT_TRAFFIC = {"gi_temporal": 153.9e6}
+DOMINANT_TRAFFIC = {"gi_temporal": 165.4e6}
 SIDE_STREAM_PASSES = ("shadow", "specular")
 CACHE_TRAIN_FRAMES = 60    # online training before the radiance-cache form is timed
 WORKLOAD = ("1920x1080 frame, seeded 1M-triangle city scene, GI 1/2 res + DI + specular GI + SVGF x5 + TAA + AgX "
