@@ -1782,12 +1782,13 @@ __global__ void __launch_bounds__(128) giFromCacheKernel(const RestirParams P, B
 	storeH4(moments, i, v4(l, l * l, 1.0f, 0.0f));
 }
 
-// Training: sample j starts at a seeded GI pixel's G-buffer surface and
-// traces one cosine-distributed suffix ray.
-__global__ void __launch_bounds__(128) trainingRaysKernel(const RestirParams P, BvhView bvh, GiBindings b, CacheWorkspace c)
+// Training: sample j < count starts at a seeded GI pixel's G-buffer surface
+// and traces one cosine-distributed suffix ray.
+__global__ void __launch_bounds__(128) trainingRaysKernel(const RestirParams P, BvhView bvh, GiBindings b, CacheWorkspace c,
+	uint32_t count)
 {
 	const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-	if (j >= c.samples)
+	if (j >= count)
 	{
 		return;
 	}
@@ -1814,12 +1815,13 @@ __global__ void __launch_bounds__(128) trainingRaysKernel(const RestirParams P, 
 		g.diffuseAlbedo(uv));
 }
 
-// The suffix's first hit: its direct light and emission now, a query for
-// the cache's value there.
-__global__ void __launch_bounds__(128) trainingHitsKernel(const RestirParams P, BvhView bvh, GiBindings b, CacheWorkspace c)
+// The suffix's first hit (rows begin..end-1): its direct light and emission
+// now, a query for the cache's value there.
+__global__ void __launch_bounds__(128) trainingHitsKernel(const RestirParams P, BvhView bvh, GiBindings b, CacheWorkspace c,
+	uint32_t begin, uint32_t end)
 {
-	const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-	if (j >= c.samples)
+	const uint32_t j = begin + blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= end)
 	{
 		return;
 	}
@@ -1852,6 +1854,39 @@ __global__ void __launch_bounds__(128) trainingHitsKernel(const RestirParams P, 
 	}
 	c.partial[j] = make_float4(light.x, light.y, light.z, weight);
 	c.hitAlbedo[j] = make_float4(albedo.x, albedo.y, albedo.z, 0.0f);
+}
+
+// The second half of the training rows: row first + j starts where row j's
+// suffix hit (the point a GI sample of a visible surface lands on, and where
+// the GI passes query the cache), with that hit's query (its surface, the
+// direction back toward row j's point), and traces its own cosine-distributed
+// suffix. Rows whose first suffix left the scene are padding (weight 0).
+__global__ void __launch_bounds__(128) trainingSecondRaysKernel(const RestirParams P, BvhView bvh, GiBindings b,
+	CacheWorkspace c, uint32_t first, uint32_t count)
+{
+	const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= count)
+	{
+		return;
+	}
+	GiPass g = makePass(P, bvh, b, P.camera_position, nullptr, 0);
+	const uint32_t row = first + j;
+	const float4* hit = c.hitQueries + size_t(j) * 4;
+	float4* query = c.trainQueries + size_t(row) * 4;
+	const bool valid = hit[1].w > 0.5f;
+	for (int k = 0; k < 4; ++k)
+	{
+		query[k] = hit[k];
+	}
+	uint32_t rng = pcg(row + pcg(uint32_t(P.frame_index) ^ 0x2545f491u));
+	const float r0 = nextRandom(rng);
+	const float r1 = nextRandom(rng);
+	const V3 position = v3(hit[0].x, hit[0].y, hit[0].z);
+	const V3 normal = v3(hit[1].x, hit[1].y, hit[1].z);
+	const V3 direction = valid ? GiPass::cosineHemisphere(normal, r0, r1) : normal;
+	const V3 origin = position + normal * g.kRayBias();
+	c.trainQueue.rays[2 * row] = make_float4(origin.x, origin.y, origin.z, valid ? g.kMaxBvhRayDistance() : 0.0f);
+	c.trainQueue.rays[2 * row + 1] = make_float4(direction.x, direction.y, direction.z, 0.0f);
 }
 
 // The training target: the light arriving along the suffix, i.e. its hit's
@@ -2050,10 +2085,32 @@ extern "C" int restir_cache_train_frame(const RestirParams* params, const Restir
 	b.shadowAtlas = shadow_atlas;
 	const BvhView bvh = makeBvhView(scene);
 	cudaStream_t s = asStream(stream);
+	// Rows [0, first): points on visible surfaces; rows [first, samples): the
+	// first suffix hits of rows [0, samples - first), so the cache also learns
+	// at the points the GI passes query it (the GI samples' surfaces, mostly
+	// off screen), which a cache trained on visible surfaces alone only
+	// extrapolates to. Each row traces one ray: the frame's ray budget is the
+	// same as with visible-surface rows only.
+	const uint32_t first = (c.samples + 1u) / 2u;
+	const uint32_t second = c.samples - first;
+	RayQueue firstQueue = c.trainQueue;
+	firstQueue.capacity = first;
+	RayQueue secondQueue = c.trainQueue;
+	secondQueue.rays = c.trainQueue.rays + 2 * size_t(first);
+	secondQueue.hitTriangle = c.trainQueue.hitTriangle + first;
+	secondQueue.hitDistance = c.trainQueue.hitDistance + first;
+	secondQueue.capacity = second;
 	cudaMemsetAsync(c.trainQueue.claimed, 0, sizeof(uint32_t), s);
-	trainingRaysKernel<<<gridFor(c.samples), 128, 0, s>>>(*params, bvh, b, c);
-	traceQueueKernel<<<persistentBlocks(), 128, 0, s>>>(bvh, c.trainQueue);
-	trainingHitsKernel<<<gridFor(c.samples), 128, 0, s>>>(*params, bvh, b, c);
+	trainingRaysKernel<<<gridFor(first), 128, 0, s>>>(*params, bvh, b, c, first);
+	traceQueueKernel<<<persistentBlocks(), 128, 0, s>>>(bvh, firstQueue);
+	trainingHitsKernel<<<gridFor(first), 128, 0, s>>>(*params, bvh, b, c, 0u, first);
+	if (second > 0u)
+	{
+		trainingSecondRaysKernel<<<gridFor(second), 128, 0, s>>>(*params, bvh, b, c, first, second);
+		cudaMemsetAsync(c.trainQueue.claimed, 0, sizeof(uint32_t), s);
+		traceQueueKernel<<<persistentBlocks(), 128, 0, s>>>(bvh, secondQueue);
+		trainingHitsKernel<<<gridFor(second), 128, 0, s>>>(*params, bvh, b, c, first, c.samples);
+	}
 	int status = restir_cache_query(cache_config, cache_state, reinterpret_cast<const float*>(c.hitQueries), c.samples,
 		c.hitValues, stream);
 	if (status != RESTIR_OK)
