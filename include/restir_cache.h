@@ -201,12 +201,16 @@ int restir_gi_from_cache(const RestirParams* params, const RestirScene* scene, c
 	const RestirCacheConfig* cache_config, const void* cache_state, void* workspace, uint64_t workspace_bytes,
 	const RestirGiReservoirs* output, uint16_t* color, uint16_t* moments, void* stream);
 
-/* One training step on params->cache_training_samples path suffixes: each
- * starts at a seeded GI pixel's G-buffer surface, takes a cosine-distributed
- * direction and its first hit through the BVH; the target is the light
- * leaving that hit toward the start (point light with the shadow atlas, the
- * triangle's emission, the sky on a miss) plus the hit's albedo times the
- * cache's own value there. */
+/* One training step on params->cache_training_samples path suffixes. Half of
+ * them start at seeded GI pixels' G-buffer surfaces; the other half start at
+ * the first hits of the previous frame's call's suffixes (where the GI
+ * passes query the cache), which the workspace keeps between calls: pass the
+ * same workspace every frame. Rows the previous call did not write (the first
+ * call, another frame index than the previous one + 1) are padding. Each takes
+ * a cosine-distributed direction and its first hit through the BVH; the
+ * target is the light leaving that hit toward the start (point light with the
+ * shadow atlas, the triangle's emission, the sky on a miss) plus the hit's
+ * albedo times the cache's own value there. */
 int restir_cache_train_frame(const RestirParams* params, const RestirScene* scene, const RestirGBuffer* gbuffer,
 	const float* shadow_atlas, const RestirCacheConfig* cache_config, void* cache_state, void* workspace,
 	uint64_t workspace_bytes, void* stream);

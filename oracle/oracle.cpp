@@ -392,6 +392,10 @@ struct TemporalThread
 
 } // namespace
 
+/* The largest reservoir weight the temporal pass with the radiance cache
+ * stores (restir_gi_temporal_cached's cap). */
+static const float kCachedReservoirWeightCap = 64.0f;
+
 /* cache_values (half4 per slot, null for the plain pass): the radiance
  * cache's values for the candidates (slot pixel * initial_candidates + k)
  * then last frame's reservoirs (slot GI pixels * initial_candidates + pixel),
@@ -592,6 +596,12 @@ const int threadCount = threads();
 					{
 						t.combinedWeight *= limit / t.estimate;
 					}
+				}
+				if (g.cache != nullptr)
+				{
+					// The form with the radiance cache (no reference counterpart) caps
+					// the stored reservoir weight, as restir_gi_temporal_cached does.
+					t.combinedWeight = fminf(t.combinedWeight, kCachedReservoirWeightCap);
 				}
 				if (t.inside)
 				{
