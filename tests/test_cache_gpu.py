@@ -230,6 +230,12 @@ def test_renderer_cache_forms_train_on_a_side_stream(cache_only):
     raw = rb.device_view(pointer, nbytes, torch.uint8)[layout.scalars:layout.scalars + 64].cpu().numpy()
     scalars = rb.abi.RestirCacheScalars.from_buffer_copy(raw[:C.sizeof(rb.abi.RestirCacheScalars)].tobytes())
     assert scalars.step == 6
+    if not cache_only:
+        # The GI passes with the cache store no reservoir weight above 64.
+        gi_pixels = params.gi_width * params.gi_height
+        for name in ("gi.receiver0", "gi.receiver1"):
+            weights = renderer.download(name, np.float32)[:4 * gi_pixels].reshape(-1, 4)[:, 3]
+            assert np.all(np.isfinite(weights)) and weights.max() <= 64.0, name
 
 
 @pytest.mark.gpu
