@@ -1896,19 +1896,26 @@ __global__ void __launch_bounds__(128) trainingSecondRaysKernel(const RestirPara
 	const float4* hit = c.hitQueries + size_t(j) * 4;
 	float4* query = c.trainQueries + size_t(row) * 4;
 	const bool valid = hit[1].w > 0.5f && __float_as_uint(hit[3].w) == uint32_t(P.frame_index);
+	if (!valid)
+	{
+		// A padding row: a clean query (whatever the workspace held) and an empty ray.
+		writeQuery(query, v3s(0.0f), 0.0f, v3(0.0f, 0.0f, 1.0f), false, v3(0.0f, 0.0f, 1.0f), v3s(0.0f));
+		c.trainQueue.rays[2 * row] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+		c.trainQueue.rays[2 * row + 1] = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
+		return;
+	}
 	for (int k = 0; k < 4; ++k)
 	{
 		query[k] = hit[k];
 	}
-	query[1].w = valid ? 1.0f : 0.0f;
 	uint32_t rng = pcg(row + pcg(uint32_t(P.frame_index) ^ 0x2545f491u));
 	const float r0 = nextRandom(rng);
 	const float r1 = nextRandom(rng);
 	const V3 position = v3(hit[0].x, hit[0].y, hit[0].z);
 	const V3 normal = v3(hit[1].x, hit[1].y, hit[1].z);
-	const V3 direction = valid ? GiPass::cosineHemisphere(normal, r0, r1) : normal;
+	const V3 direction = GiPass::cosineHemisphere(normal, r0, r1);
 	const V3 origin = position + normal * g.kRayBias();
-	c.trainQueue.rays[2 * row] = make_float4(origin.x, origin.y, origin.z, valid ? g.kMaxBvhRayDistance() : 0.0f);
+	c.trainQueue.rays[2 * row] = make_float4(origin.x, origin.y, origin.z, g.kMaxBvhRayDistance());
 	c.trainQueue.rays[2 * row + 1] = make_float4(direction.x, direction.y, direction.z, 0.0f);
 }
 
